@@ -1,0 +1,398 @@
+"""Benchmark: classic label propagation, GTEPS per iteration, R-MAT scale 24.
+
+Workload (the reference's headline configuration for this path): R-MAT
+scale 24 (16.8M vertices), edge factor 16, a/b/c/d = .57/.19/.19/.05,
+seed 2, symmetrised, self loops and duplicates removed, degree-descending
+relabel, int32 CSR; classic LP (method 1), labels = vertex ids at the start,
+20 synchronous iterations.  A bench "step" is one such 20-iteration run over
+the device-resident graph.  GTEPS = CSR entries x iterations / seconds.
+
+* value: device time (CUDA events on the launching stream) of K steps with
+  the graph already in HBM; the CSR (~1.9 GB) is larger than L2, so no
+  explicit flush is done between steps.
+* e2e: the same metric through the public API with host buffers: every step
+  copies the CSR from pinned host memory (glp_graph_create), runs, and reads
+  the labels back to the host.
+* roofline: the dominant kernel tier, algorithmic bytes 8*m_t + 12*n_t per
+  launch over its CUDA-event launch time, against the measured HBM copy peak.
+* cpu_baseline: the reference's own OpenMP CPU path (tutorial/CPUlp.cuh,
+  compiled from source into oracle/_ref) on the same graph, one iteration.
+
+Multi-GPU: each rank runs an independent replica (the path does not shard
+across GPUs); value = total edges*iterations of all ranks / max rank time.
+
+--impl reference times the reference's own CPU implementation instead
+(rank 0 only), one LP iteration per step on the same graph.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+ITERS = 20
+TIER_NAMES = ("tiny", "group16", "group32", "mid", "big", "hub", "aux", "-")
+TIER_PLAN_KEYS = ("tiny", "group16", "group32", "mid", "big", "hub")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="glp", choices=["glp", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--iters", type=int, default=ITERS)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-iters", type=int, default=1)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- distributed
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.proc = None
+        self.lines: list[str] = []
+        try:
+            uuid = str(torch.cuda.get_device_properties(device).uuid)
+            ident = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+        except Exception:
+            ident = str(device)
+        self.cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                    "-i", ident]
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(self.cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch per kernel tier from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ----------------------------------------------------------------- workload
+def make_graph(scale: int, seed: int, device):
+    from glp_b200 import graphs
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = graphs.rmat(scale, 16, seed=seed, device=device)
+    torch.cuda.synchronize()
+    return g, time.perf_counter() - t0
+
+
+def write_csr(path: str, off: np.ndarray, cols: np.ndarray):
+    with open(path, "wb") as f:
+        np.array([len(off) - 1, len(cols)], dtype=np.int64).tofile(f)
+        off.astype(np.int32).tofile(f)
+        cols.astype(np.int32).tofile(f)
+
+
+def ref_cpulp_run(csr_path: str, niter: int, threads: int | None = None):
+    """Run the reference CPUlp::sync_run_1 (oracle/_ref/ref_cpulp) and return
+    its per-iteration seconds as printed by the reference."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_cpulp")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    env = dict(os.environ)
+    if threads:
+        env["OMP_THREAD_LIMIT"] = str(threads)
+    with tempfile.TemporaryDirectory() as d:
+        r = subprocess.run([exe, "sync-csr", csr_path, str(niter), os.path.join(d, "l.bin")], capture_output=True,
+                           text=True, env=env, check=True)
+    return [float(x) for x in re.findall(r"t1: ([0-9.eE+-]+)", r.stdout)]
+
+
+def cpu_threads_used() -> int:
+    # CPUlp.cuh:50 hard-codes num_threads(20); the OpenMP runtime may cap it
+    lim = os.environ.get("OMP_THREAD_LIMIT")
+    return min(20, int(lim)) if lim else 20
+
+
+# ----------------------------------------------------------------- arms
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_cpulp")):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_cpulp was not built"}))
+        return
+    g, _ = make_graph(args.scale, args.seed, "cuda")
+    off, cols, _ = g.numpy()
+    n, m = len(off) - 1, len(cols)
+    del g
+    torch.cuda.empty_cache()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "g.csr")
+        write_csr(path, off, cols)
+        times = ref_cpulp_run(path, args.warmup + args.steps)
+    timed = times[args.warmup:]
+    t = sum(timed)
+    value = m * len(timed) / t / 1e9
+    cores = cpu_threads_used()
+    sample = (f"CPUlp::sync_run_1 on the full R-MAT s{args.scale} graph (n={n}, m={m}); steps = reference LP "
+              f"iterations {args.warmup}..{args.warmup + args.steps - 1} after {args.warmup} warm-up iterations")
+    line = {
+        "metric": f"classic LP GTEPS per iteration, R-MAT scale {args.scale}", "value": round(value, 4),
+        "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * t / len(timed), 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the box",
+        "config": {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic", "n": n, "m": m,
+                   "step": "one reference CPU iteration"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_glp(args, ws, rank, local):
+    from glp_b200 import _lib
+    from glp_b200.engine import Graph, make_params
+    from glp_b200.graphs import CSR
+
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    g, gen_s = make_graph(args.scale, args.seed, dev)
+    n, m = g.n, g.m
+    params = make_params()
+    handle = Graph(g)
+    plan = handle.plan(params)
+    labels_dev = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    for _ in range(args.warmup):
+        handle.run(_lib.METHOD_CLASSIC, args.iters, params, labels_out=labels_dev, stream=sp)
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    tier_ms = np.zeros(8)
+    launches = 0
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        r = handle.run(_lib.METHOD_CLASSIC, args.iters, params, labels_out=labels_dev, stream=sp, profile=True)
+        tier_ms += r.tier_ms
+        launches += r.launches
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ws, ms)
+    edges_total = sum_over_ranks(ws, float(m) * args.iters * args.steps)
+    value = edges_total / (ms_max / 1e3) / 1e9
+
+    # end to end through the public API with host buffers
+    off_h = g.offsets.cpu().pin_memory()
+    cols_h = g.cols.cpu().pin_memory()
+    host_csr = CSR(off_h, cols_h)
+    lab_h = None
+    for _ in range(1):  # warm the host path once
+        h2 = Graph(host_csr)
+        lab_h = h2.run(_lib.METHOD_CLASSIC, args.iters, params).labels
+        h2.close()
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        h2 = Graph(host_csr)
+        lab_h = h2.run(_lib.METHOD_CLASSIC, args.iters, params).labels
+        h2.close()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    e2e_edges = sum_over_ranks(ws, float(m) * args.iters * args.e2e_steps)
+    e2e_value = e2e_edges / (e2e_ms / 1e3) / 1e9
+    same = bool(np.array_equal(lab_h, labels_dev.cpu().numpy()))
+
+    # roofline of the dominant kernel tier
+    peak, peak_kind = measured_peak()
+    launches_per_tier = args.steps * args.iters
+    dom = int(np.argmax(tier_ms[:6]))
+    key = TIER_PLAN_KEYS[dom]
+    n_t, m_t = plan[f"v_{key}"], plan[f"e_{key}"]
+    bytes_launch = 8 * m_t + 12 * n_t
+    avg_ms = tier_ms[dom] / launches_per_tier
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    traffic = profiled_traffic().get(key)
+    total_bytes_iter = 8 * m + 12 * n + 4
+    iter_ms = ms / (args.steps * args.iters)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            off_np, cols_np = off_h.numpy(), cols_h.numpy()
+            with tempfile.TemporaryDirectory() as d:
+                path = os.path.join(d, "g.csr")
+                write_csr(path, off_np, cols_np)
+                times = ref_cpulp_run(path, args.cpu_iters)
+            tcpu = sum(times)
+            cpu = {"value": round(m * len(times) / tcpu / 1e9, 4), "unit": "GTEPS", "cores": cpu_threads_used(),
+                   "kind": "reference",
+                   "sample": f"reference CPUlp::sync_run_1 (tutorial/CPUlp.cuh, built from source), "
+                             f"{len(times)} iteration(s) on the full graph, {tcpu:.2f} s; host has "
+                             f"{os.cpu_count()} cpus"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GTEPS", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": f"classic LP GTEPS per iteration, R-MAT scale {args.scale}",
+            "value": round(value, 3), "unit": "GTEPS", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the GPU",
+            "config": {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic-{args.iters}it", "n": n, "m": m,
+                       "iterations_per_step": args.iters, "parallelism": f"replicas{ws}",
+                       "l2": "inputs larger than L2 (CSR %.2f GB); no flush" % ((4 * (n + 1 + m)) / 1e9),
+                       "graph_gen_s": round(gen_s, 2)},
+            "e2e": {"value": round(e2e_value, 3), "unit": "GTEPS", "h2d_bytes_per_step": int(4 * (n + 1 + m)),
+                    "d2h_bytes_per_step": int(4 * n), "steps": args.e2e_steps, "labels_match_device_run": same},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": f"k_{key}",
+                         "peak_kind": peak_kind, "bytes_per_launch": int(bytes_launch),
+                         "avg_launch_ms": round(avg_ms, 4)},
+            "whole_step_roofline": {"bytes_per_iter": int(total_bytes_iter), "iter_ms": round(iter_ms, 4),
+                                    "achieved_gbs": round(total_bytes_iter / (iter_ms / 1e3) / 1e9, 1),
+                                    "frac": round(total_bytes_iter / (iter_ms / 1e3) / 1e9 / peak, 4)},
+            "tier_ms_per_iter": {TIER_NAMES[i]: round(tier_ms[i] / launches_per_tier, 4) for i in range(6)},
+            "plan": plan,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    handle.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_glp(args, ws, rank, local)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,122 @@
+// device.cuh -- device helpers shared by the label-propagation kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace glp {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+// Error bits a kernel may raise in the per-handle status word (never traps).
+enum : uint32_t {
+  kErrProbe = 1u,       // a hash table probe ran past its capacity
+  kErrScoreRange = 2u,  // a layered score left the packable range
+  kErrHubPlan = 4u,     // hub chunk bookkeeping inconsistent
+};
+
+// Murmur3 fmix32 finaliser; the reference hashes labels with it too
+// (method/hashtable.cuh:19-26).
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t k) {
+  k ^= k >> 16;
+  k *= 0x85ebca6bu;
+  k ^= k >> 13;
+  k *= 0xc2b2ae35u;
+  k ^= k >> 16;
+  return k;
+}
+
+// SplitMix64 finaliser (Steele, Lea, Flood, OOPSLA 2014).
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+// SLPA speaker hash H(seed, iter, v).
+__host__ __device__ __forceinline__ uint64_t slpa_hash(uint64_t seed, uint32_t iter, uint32_t v) {
+  return mix64(mix64(mix64(seed) ^ (uint64_t)iter) ^ (uint64_t)v);
+}
+
+// Streaming load for data read once per iteration (CSR columns, weights).
+__device__ __forceinline__ int32_t ld_stream(const int32_t* p) { return __ldcs(p); }
+// Read-only cached load for the label gather (reused across edges).
+__device__ __forceinline__ int32_t ld_label(const int32_t* p) { return __ldg(p); }
+
+// A (score, label) candidate; larger score wins, then larger label.
+struct Best {
+  int64_t s;
+  int32_t l;
+};
+__device__ __forceinline__ Best best_none() { return Best{INT64_MIN, -1}; }
+__device__ __forceinline__ bool better(const Best& a, const Best& b) {
+  return a.s > b.s || (a.s == b.s && a.l > b.l);
+}
+__device__ __forceinline__ Best shfl_xor_best(const Best& b, int m) {
+  Best o;
+  o.s = __shfl_xor_sync(kFull, b.s, m);
+  o.l = __shfl_xor_sync(kFull, b.l, m);
+  return o;
+}
+// Max over aligned groups of G lanes (G power of two, <= 32).
+template <int G>
+__device__ __forceinline__ Best group_max(Best b) {
+#pragma unroll
+  for (int m = G / 2; m >= 1; m >>= 1) {
+    Best o = shfl_xor_best(b, m);
+    if (better(o, b)) b = o;
+  }
+  return b;
+}
+
+// Block-wide max; every thread gets the result.  scratch: >= 32 Best.
+template <int NT>
+__device__ __forceinline__ Best block_max(Best b, Best* scratch) {
+  b = group_max<32>(b);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) scratch[warp] = b;
+  __syncthreads();
+  if (warp == 0) {
+    Best x = lane < NT / 32 ? scratch[lane] : best_none();
+    x = group_max<32>(x);
+    if (lane == 0) scratch[0] = x;
+  }
+  __syncthreads();
+  Best r = scratch[0];
+  __syncthreads();
+  return r;
+}
+
+// Open-addressing counter table (linear probing) in shared or global memory:
+// keys hold label+1 (0 = empty), vals the running count or weight sum.
+// insert() returns the count AFTER adding c; the largest value returned for a
+// key over all of its inserts is its final total, whatever the order.
+struct CountTable {
+  uint32_t* keys;
+  uint32_t* vals;
+  uint32_t mask;  // capacity - 1, capacity a power of two
+
+  __device__ __forceinline__ uint32_t insert(uint32_t key, uint32_t c, uint32_t* err) const {
+    uint32_t h = fmix32(key) & mask;
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      uint32_t cur = keys[h];
+      if (cur == 0) {
+        uint32_t prev = atomicCAS(&keys[h], 0u, key);
+        if (prev == 0u || prev == key) return atomicAdd(&vals[h], c) + c;
+      } else if (cur == key) {
+        return atomicAdd(&vals[h], c) + c;
+      }
+      h = (h + 1) & mask;
+    }
+    atomicOr(err, kErrProbe);
+    return 0;
+  }
+};
+
+// Warp-aggregated increment of a counter.
+__device__ __forceinline__ void warp_count_add(unsigned long long* counter, bool flag) {
+  const uint32_t b = __ballot_sync(kFull, flag);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(counter, (unsigned long long)__popc(b));
+}
+
+}  // namespace glp

@@ -1,0 +1,887 @@
+// engine.cu -- graph handle, degree-tier planner, propagation drivers and the
+// C ABI of include/glp.h.
+//
+// Reference correspondence:
+//   glp_graph_create      <- CSRGraph + XProp::preprocess (header/graph.h:61-198,
+//                            prop/classicLprop.cuh:65-78)
+//   build_host_plan       <- degree binning + hub block plan + tiny packing
+//                            (prop/classicLprop.cuh:196-308, kernel.cuh:6011-6046)
+//   run_classic           <- classicLprop::perform_lp loop (prop/classicLprop.cuh:361-443)
+//   run_layered           <- MultiLprop::perform_lp loop (prop/MultiLprop.cuh:308-374)
+//   run_slpa              <- SLPA loop (tutorial/Base5prop.cuh:264-293)
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "engine.h"
+#include "hooks_engine.cuh"
+
+namespace glp {
+
+int validate_csr_device(glp_graph* g);
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? GLP_ENOMEM : GLP_ECUDA;
+}
+
+static int require_device() {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    set_error("no usable CUDA device (%s)", e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+    return GLP_ENODEV;
+  }
+  return GLP_OK;
+}
+
+static uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+int resolve_tiers(const glp_params* p, TierParams* t) {
+  TierParams d;
+  if (p) {
+    if (p->tiny_max > 0) d.tiny_max = p->tiny_max;
+    if (p->tiny_max < 0) d.tiny_max = 0;
+    if (p->mid_max > 0) d.mid_max = p->mid_max;
+    if (p->big_max > 0) d.big_max = p->big_max;
+    if (p->hub_chunk > 0) d.hub_chunk = p->hub_chunk;
+  }
+  if (d.tiny_max > 8) {
+    set_error("tiny_max %d > 8", d.tiny_max);
+    return GLP_EINVAL;
+  }
+  if (d.mid_max < 32 || d.mid_max > 256) {
+    set_error("mid_max %d outside [32, 256]", d.mid_max);
+    return GLP_EINVAL;
+  }
+  if (d.big_max < d.mid_max || d.big_max > 8192) {
+    set_error("big_max %d outside [mid_max, 8192]", d.big_max);
+    return GLP_EINVAL;
+  }
+  if (d.hub_chunk < 256 || d.hub_chunk > 8192) {
+    set_error("hub_chunk %d outside [256, 8192]", d.hub_chunk);
+    return GLP_EINVAL;
+  }
+  *t = d;
+  return GLP_OK;
+}
+
+void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPlan* hp) {
+  *hp = HostPlan{};
+  for (int32_t v = 0; v < n; ++v) {
+    const int32_t d = off[v + 1] - off[v];
+    if (d == 0) {
+      hp->isolated++;
+    } else if (d <= t.tiny_max) {
+      hp->tiny.push_back(v);
+    } else if (d <= 16) {
+      hp->g16.push_back(v);
+    } else if (d <= 32) {
+      hp->g32.push_back(v);
+    } else if (d <= t.mid_max) {
+      hp->mid.push_back(v);
+    } else if (d <= t.big_max) {
+      hp->big.push_back(v);
+    } else {
+      const int32_t h = (int32_t)hp->hub_v.size();
+      const int32_t nch = (d + t.hub_chunk - 1) / t.hub_chunk;
+      hp->hub_v.push_back(v);
+      hp->hub_nchunks.push_back(nch);
+      const uint64_t cap = next_pow2(2ull * (uint64_t)d);
+      hp->hub_tbase.push_back(hp->table_slots);
+      hp->hub_tmask.push_back((uint32_t)(cap - 1));
+      hp->table_slots += (int64_t)cap;
+      hp->hub_ubase.push_back(hp->used_slots);
+      hp->used_slots += d;
+      for (int32_t c = 0; c < nch; ++c) {
+        hp->chunk_hub.push_back(h);
+        hp->chunk_begin.push_back(off[v] + c * t.hub_chunk);
+        hp->chunk_end.push_back(std::min(off[v + 1], off[v] + (c + 1) * t.hub_chunk));
+      }
+    }
+  }
+}
+
+static void free_plan(DevicePlan* p) {
+  for (void* a : p->allocs) cudaFree(a);
+  *p = DevicePlan{};
+}
+
+template <class T>
+static int upload(DevicePlan* p, const std::vector<T>& v, T** out) {
+  *out = nullptr;
+  if (v.empty()) return GLP_OK;
+  void* d = nullptr;
+  GLP_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+  p->allocs.push_back(d);
+  GLP_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = static_cast<T*>(d);
+  return GLP_OK;
+}
+
+template <class T>
+static int zeroed(DevicePlan* p, size_t count, T** out) {
+  *out = nullptr;
+  if (count == 0) return GLP_OK;
+  void* d = nullptr;
+  GLP_CUDA(cudaMalloc(&d, count * sizeof(T)));
+  p->allocs.push_back(d);
+  GLP_CUDA(cudaMemset(d, 0, count * sizeof(T)));
+  *out = static_cast<T*>(d);
+  return GLP_OK;
+}
+
+static int ensure_plan(glp_graph* g, const TierParams& t) {
+  if (g->plan.valid && g->plan.tiers == t) return GLP_OK;
+  free_plan(&g->plan);
+  HostPlan hp;
+  build_host_plan(g->h_off.data(), g->n, t, &hp);
+  DevicePlan& p = g->plan;
+  p.tiers = t;
+  p.isolated = hp.isolated;
+  int rc;
+  if ((rc = upload(&p, hp.tiny, &p.tiny)) || (rc = upload(&p, hp.g16, &p.g16)) || (rc = upload(&p, hp.g32, &p.g32)) ||
+      (rc = upload(&p, hp.mid, &p.mid)) || (rc = upload(&p, hp.big, &p.big))) {
+    free_plan(&p);
+    return rc;
+  }
+  p.n_tiny = (int32_t)hp.tiny.size();
+  p.n_g16 = (int32_t)hp.g16.size();
+  p.n_g32 = (int32_t)hp.g32.size();
+  p.n_mid = (int32_t)hp.mid.size();
+  p.n_big = (int32_t)hp.big.size();
+  p.n_hubs = (int32_t)hp.hub_v.size();
+  p.n_chunks = (int32_t)hp.chunk_hub.size();
+  p.big_cap = (uint32_t)next_pow2(2ull * (uint64_t)t.big_max);
+  p.hub_cap = (uint32_t)next_pow2(2ull * (uint64_t)t.hub_chunk);
+  if (p.n_hubs) {
+    HubPlan& h = p.hub;
+    if ((rc = upload(&p, hp.chunk_hub, (int32_t**)&h.chunk_hub)) ||
+        (rc = upload(&p, hp.chunk_begin, (int32_t**)&h.chunk_begin)) ||
+        (rc = upload(&p, hp.chunk_end, (int32_t**)&h.chunk_end)) || (rc = upload(&p, hp.hub_v, (int32_t**)&h.hub_v)) ||
+        (rc = upload(&p, hp.hub_nchunks, (int32_t**)&h.hub_nchunks)) ||
+        (rc = upload(&p, hp.hub_tbase, (int64_t**)&h.hub_tbase)) ||
+        (rc = upload(&p, hp.hub_tmask, (uint32_t**)&h.hub_tmask)) ||
+        (rc = upload(&p, hp.hub_ubase, (int64_t**)&h.hub_ubase)) ||
+        (rc = zeroed(&p, (size_t)hp.table_slots, &h.gkeys)) || (rc = zeroed(&p, (size_t)hp.table_slots, &h.gvals)) ||
+        (rc = zeroed(&p, (size_t)hp.used_slots, &h.used)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.used_n)) ||
+        (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_best)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_done))) {
+      free_plan(&p);
+      return rc;
+    }
+  }
+  p.valid = true;
+  return GLP_OK;
+}
+
+// --------------------------------------------------------------- launches
+template <class K>
+static int allow_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) GLP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return GLP_OK;
+}
+
+static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+template <bool W, class S>
+int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t* launches) {
+  const DevicePlan& p = *L.plan;
+  cudaStream_t s = L.stream;
+  auto mark = [&](int i, int which) -> int {
+    if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[2 * i + which], s));
+    return GLP_OK;
+  };
+  int rc;
+  constexpr int kHubNT = 512, kBigNT = 512, kMidNT = 256;
+  if (p.n_hubs) {
+    const size_t sm = 2ull * p.hub_cap * sizeof(uint32_t);
+    if ((rc = allow_smem(k_hub<kHubNT, W, S>, sm))) return rc;
+    if ((rc = mark(5, 0))) return rc;
+    k_hub<kHubNT, W, S><<<p.n_chunks, kHubNT, sm, s>>>(a, p.hub, p.n_chunks, p.hub_cap, score);
+    if ((rc = mark(5, 1))) return rc;
+    ++*launches;
+  }
+  if (p.n_big) {
+    const size_t sm = 2ull * p.big_cap * sizeof(uint32_t);
+    if ((rc = allow_smem(k_big<kBigNT, W, S>, sm))) return rc;
+    if ((rc = mark(4, 0))) return rc;
+    k_big<kBigNT, W, S><<<p.n_big, kBigNT, sm, s>>>(a, p.big, p.n_big, p.big_cap, score);
+    if ((rc = mark(4, 1))) return rc;
+    ++*launches;
+  }
+  if (p.n_mid) {
+    if ((rc = mark(3, 0))) return rc;
+    k_mid<512, kMidNT, W, S><<<(unsigned)cdiv(p.n_mid, kMidNT / 32), kMidNT, 0, s>>>(a, p.mid, p.n_mid, score);
+    if ((rc = mark(3, 1))) return rc;
+    ++*launches;
+  }
+  if (p.n_g32) {
+    if ((rc = mark(2, 0))) return rc;
+    k_group<32, W, S><<<(unsigned)cdiv((int64_t)p.n_g32 * 32, 256), 256, 0, s>>>(a, p.g32, p.n_g32, score);
+    if ((rc = mark(2, 1))) return rc;
+    ++*launches;
+  }
+  if (p.n_g16) {
+    if ((rc = mark(1, 0))) return rc;
+    k_group<16, W, S><<<(unsigned)cdiv((int64_t)p.n_g16 * 16, 256), 256, 0, s>>>(a, p.g16, p.n_g16, score);
+    if ((rc = mark(1, 1))) return rc;
+    ++*launches;
+  }
+  if (p.n_tiny) {
+    if ((rc = mark(0, 0))) return rc;
+    k_tiny<8, W, S><<<(unsigned)cdiv(p.n_tiny, 256), 256, 0, s>>>(a, p.tiny, p.n_tiny, score);
+    if ((rc = mark(0, 1))) return rc;
+    ++*launches;
+  }
+  GLP_CUDA(cudaGetLastError());
+  return GLP_OK;
+}
+
+// ------------------------------------------------------------ run context
+// Per-tier device timing: every step gets its own 16 events (start/stop for 8
+// tiers), recorded on the run's stream around each kernel and read once after
+// the run, so timing adds no host synchronisation inside the loop.
+struct RunCtx {
+  glp_graph* g = nullptr;
+  cudaStream_t s = nullptr;
+  glp_iter_cb cb = nullptr;
+  void* user = nullptr;
+  std::vector<int32_t> hbuf;
+  bool timing = false;
+  std::vector<std::vector<cudaEvent_t>> evs;
+  std::vector<std::vector<bool>> ran;
+  size_t used = 0;
+  float tier_ms[8] = {};
+  int64_t launches = 0;
+  int iter_base = 0;
+
+  ~RunCtx() {
+    for (auto& v : evs)
+      for (cudaEvent_t e : v)
+        if (e) cudaEventDestroy(e);
+  }
+  // Events for the next step (nullptr when not timing).
+  cudaEvent_t* step_events() {
+    if (!timing) return nullptr;
+    if (used == evs.size()) {
+      std::vector<cudaEvent_t> v(16, nullptr);
+      for (auto& e : v)
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      evs.push_back(v);
+    }
+    ran.emplace_back(8, false);
+    return evs[used++].data();
+  }
+  void mark_ran(int tier) {
+    if (timing && !ran.empty()) ran.back()[tier] = true;
+  }
+  StepLaunch launch() {
+    cudaEvent_t* ev = step_events();
+    if (ev) {
+      const DevicePlan& p = g->plan;
+      ran.back()[0] = p.n_tiny > 0;
+      ran.back()[1] = p.n_g16 > 0;
+      ran.back()[2] = p.n_g32 > 0;
+      ran.back()[3] = p.n_mid > 0;
+      ran.back()[4] = p.n_big > 0;
+      ran.back()[5] = p.n_hubs > 0;
+    }
+    return StepLaunch{&g->plan, s, ev};
+  }
+  cudaEvent_t* current() { return timing && used ? evs[used - 1].data() : nullptr; }
+  int harvest() {
+    if (!timing) return GLP_OK;
+    GLP_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < used; ++i)
+      for (int t = 0; t < 8; ++t) {
+        if (!ran[i][t]) continue;
+        float ms = 0;
+        GLP_CUDA(cudaEventElapsedTime(&ms, evs[i][2 * t], evs[i][2 * t + 1]));
+        tier_ms[t] += ms;
+      }
+    return GLP_OK;
+  }
+  // Record the aux-kernel events (tier 6) of the current step.
+  int aux_mark(int which) {
+    cudaEvent_t* ev = current();
+    if (!ev) return GLP_OK;
+    GLP_CUDA(cudaEventRecord(ev[12 + which], s));
+    if (which == 1) mark_ran(6);
+    return GLP_OK;
+  }
+};
+
+static int check_err(glp_graph* g, cudaStream_t s) {
+  uint32_t err = 0;
+  GLP_CUDA(cudaMemcpyAsync(&err, g->d_err, sizeof err, cudaMemcpyDeviceToHost, s));
+  GLP_CUDA(cudaStreamSynchronize(s));
+  if (err) {
+    GLP_CUDA(cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), s));
+    GLP_CUDA(cudaStreamSynchronize(s));
+    set_error("kernel error flags 0x%x (probe overflow=1, score range=2, hub plan=4)", err);
+    return GLP_EKERNEL;
+  }
+  return GLP_OK;
+}
+
+static int after_iter(RunCtx& c, int32_t iter, const int32_t* d_labels) {
+  int rc;
+  if (!c.cb) return GLP_OK;
+  c.hbuf.resize(c.g->n);
+  GLP_CUDA(cudaMemcpyAsync(c.hbuf.data(), d_labels, sizeof(int32_t) * c.g->n, cudaMemcpyDeviceToHost, c.s));
+  if ((rc = check_err(c.g, c.s))) return rc;
+  if (c.cb(iter, c.hbuf.data(), c.g->n, c.user)) {
+    set_error("run stopped by the iteration callback at iteration %d", iter);
+    return GLP_ECANCELED;
+  }
+  return GLP_OK;
+}
+
+static int grow(int32_t** p, int64_t* have, int64_t need) {
+  if (*have >= need && *p) return GLP_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  GLP_CUDA(cudaMalloc(p, std::max<int64_t>(need, 1) * sizeof(int32_t)));
+  *have = need;
+  return GLP_OK;
+}
+
+static int ensure_work(glp_graph* g, int32_t total_iters) {
+  if (!g->d_lab[0]) {
+    GLP_CUDA(cudaMalloc(&g->d_lab[0], sizeof(int32_t) * std::max(g->n, 1)));
+    GLP_CUDA(cudaMalloc(&g->d_lab[1], sizeof(int32_t) * std::max(g->n, 1)));
+  }
+  if (!g->d_err) {
+    GLP_CUDA(cudaMalloc(&g->d_err, sizeof(uint32_t)));
+    GLP_CUDA(cudaMemset(g->d_err, 0, sizeof(uint32_t)));
+  }
+  if (g->changed_cap < total_iters + 1) {
+    if (g->d_changed) cudaFree(g->d_changed);
+    g->d_changed = nullptr;
+    GLP_CUDA(cudaMalloc(&g->d_changed, sizeof(unsigned long long) * (total_iters + 1)));
+    g->changed_cap = total_iters + 1;
+  }
+  return GLP_OK;
+}
+
+static int init_labels(RunCtx& c) {
+  glp_graph* g = c.g;
+  if (g->n == 0) return GLP_OK;
+  k_iota<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(g->d_lab[0], g->d_lab[1], g->n);
+  ++c.launches;
+  GLP_CUDA(cudaGetLastError());
+  return GLP_OK;
+}
+
+template <bool W>
+static int run_classic(RunCtx& c, int32_t niter) {
+  glp_graph* g = c.g;
+  int rc = init_labels(c);
+  if (rc) return rc;
+  for (int32_t it = 0; it < niter; ++it) {
+    StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_lab[it & 1], g->d_lab[it & 1], g->d_lab[(it + 1) & 1],
+               g->d_changed + it, g->d_err};
+    if ((rc = launch_step<W>(c.launch(), a, ScoreClassic{}, &c.launches))) return rc;
+    if ((rc = after_iter(c, it, g->d_lab[(it + 1) & 1]))) return rc;
+  }
+  return GLP_OK;
+}
+
+template <bool W>
+static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
+  glp_graph* g = c.g;
+  int64_t have0 = 0, have1 = 0;
+  int rc;
+  if (!g->d_vol[0]) {
+    if ((rc = grow(&g->d_vol[0], &have0, g->n)) || (rc = grow(&g->d_vol[1], &have1, g->n))) return rc;
+  }
+  int32_t* vol_r = g->d_vol[0];
+  int32_t* vol_w = g->d_vol[1];
+  GLP_CUDA(cudaMemsetAsync(vol_r, 0, sizeof(int32_t) * g->n, c.s));
+  GLP_CUDA(cudaMemsetAsync(vol_w, 0, sizeof(int32_t) * g->n, c.s));
+  int32_t step = 0;
+  int32_t* final_lab = g->d_lab[0];
+  for (int32_t layer = 0; layer < p.nlayers; ++layer) {
+    if ((rc = init_labels(c))) return rc;
+    for (int32_t it = 0; it < niter; ++it, ++step) {
+      if (step > 0) {
+        std::swap(vol_r, vol_w);
+        GLP_CUDA(cudaMemsetAsync(vol_w, 0, sizeof(int32_t) * g->n, c.s));
+      }
+      int32_t* lin = g->d_lab[it & 1];
+      int32_t* lout = g->d_lab[(it + 1) & 1];
+      StepArgs a{g->d_off, g->d_cols, g->d_w, lin, lin, lout, g->d_changed + step, g->d_err};
+      if ((rc = launch_step<W>(c.launch(), a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches))) return rc;
+      if ((rc = c.aux_mark(0))) return rc;
+      k_histogram<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(lout, g->n, vol_w);
+      ++c.launches;
+      if ((rc = c.aux_mark(1))) return rc;
+      GLP_CUDA(cudaGetLastError());
+      if ((rc = after_iter(c, step, lout))) return rc;
+      final_lab = lout;
+    }
+  }
+  // the final labels must sit in d_lab[0] or d_lab[1]; report which
+  c.iter_base = final_lab == g->d_lab[0] ? 0 : 1;
+  g->d_vol[0] = vol_r;
+  g->d_vol[1] = vol_w;  // vol_w = volumes after the last iteration
+  return GLP_OK;
+}
+
+template <bool W>
+static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* out) {
+  glp_graph* g = c.g;
+  const int32_t T = p.slpa_T;
+  int rc;
+  if ((rc = grow(&g->d_mem, &g->mem_elems, (int64_t)T * g->n))) return rc;
+  if (!g->d_spoken) GLP_CUDA(cudaMalloc(&g->d_spoken, sizeof(int32_t) * std::max(g->n, 1)));
+  GLP_CUDA(cudaMemsetAsync(g->d_mem, 0xff, sizeof(int32_t) * (size_t)T * g->n, c.s));
+  if ((rc = init_labels(c))) return rc;
+  for (int32_t it = 0; it < niter; ++it) {
+    int32_t* lcur = g->d_lab[it & 1];
+    int32_t* lout = g->d_lab[(it + 1) & 1];
+    StepLaunch L = c.launch();
+    if ((rc = c.aux_mark(0))) return rc;
+    k_slpa_speak<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(lcur, g->d_mem, g->d_spoken, g->n, T, it, p.seed);
+    ++c.launches;
+    if ((rc = c.aux_mark(1))) return rc;
+    GLP_CUDA(cudaGetLastError());
+    StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_spoken, lcur, lout, g->d_changed + it, g->d_err};
+    if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) return rc;
+    if ((rc = after_iter(c, it, lout))) return rc;
+  }
+  if (out->slpa_comm && g->n) {
+    const bool dev = out->on_device != 0;
+    int32_t* comm = out->slpa_comm;
+    int32_t* ncomm = out->slpa_ncomm;
+    int32_t *tmp_c = nullptr, *tmp_n = nullptr;
+    if (!dev) {
+      GLP_CUDA(cudaMalloc(&tmp_c, sizeof(int32_t) * (size_t)T * g->n));
+      GLP_CUDA(cudaMalloc(&tmp_n, sizeof(int32_t) * g->n));
+      comm = tmp_c;
+      ncomm = tmp_n;
+    }
+    k_slpa_post<64><<<(unsigned)cdiv(g->n, 128), 128, 0, c.s>>>(g->d_mem, g->n, T, p.slpa_r, comm, ncomm);
+    ++c.launches;
+    GLP_CUDA(cudaGetLastError());
+    if (!dev) {
+      GLP_CUDA(cudaMemcpyAsync(out->slpa_comm, tmp_c, sizeof(int32_t) * (size_t)T * g->n, cudaMemcpyDeviceToHost, c.s));
+      if (out->slpa_ncomm)
+        GLP_CUDA(cudaMemcpyAsync(out->slpa_ncomm, tmp_n, sizeof(int32_t) * g->n, cudaMemcpyDeviceToHost, c.s));
+      GLP_CUDA(cudaStreamSynchronize(c.s));
+      cudaFree(tmp_c);
+      cudaFree(tmp_n);
+    }
+  }
+  if (out->slpa_mem && g->n)
+    GLP_CUDA(cudaMemcpyAsync(out->slpa_mem, g->d_mem, sizeof(int32_t) * (size_t)T * g->n,
+                             out->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.s));
+  return GLP_OK;
+}
+
+// ------------------------------------------------------------ validation
+__global__ void k_validate(const int32_t* __restrict__ cols, const int32_t* __restrict__ w, int64_t m, int32_t n,
+                           uint32_t* bad) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = cols[j];
+    if (c < 0 || c >= n) atomicOr(bad, 1u);
+    if (w && w[j] < 0) atomicOr(bad, 2u);
+  }
+}
+
+int validate_csr_device(glp_graph* g) {
+  if (g->m == 0) return GLP_OK;
+  uint32_t* d_bad = nullptr;
+  GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
+  GLP_CUDA(cudaMemset(d_bad, 0, sizeof(uint32_t)));
+  k_validate<<<1184, 256>>>(g->d_cols, g->d_w, g->m, g->n, d_bad);
+  uint32_t bad = 0;
+  cudaError_t e = cudaMemcpy(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost);
+  cudaFree(d_bad);
+  if (e != cudaSuccess) return cuda_fail(e, "validate");
+  if (bad & 1u) {
+    set_error("column index outside [0, n)");
+    return GLP_EINVAL;
+  }
+  if (bad & 2u) {
+    set_error("negative edge weight");
+    return GLP_EINVAL;
+  }
+  return GLP_OK;
+}
+
+// --------------------------------------------------------------- method 4
+template <class H>
+static int hooks_iterations(RunCtx& c, H h, int32_t niter, int32_t step0, bool layered, int32_t** vol_r,
+                            int32_t** vol_w) {
+  glp_graph* g = c.g;
+  int rc;
+  for (int32_t it = 0; it < niter; ++it) {
+    const int32_t step = step0 + it;
+    if (layered) {
+      if (step > 0) {
+        std::swap(*vol_r, *vol_w);
+        GLP_CUDA(cudaMemsetAsync(*vol_w, 0, sizeof(int32_t) * g->n, c.s));
+      }
+      h.st.vol_r = *vol_r;
+      h.st.vol_w = *vol_w;
+    }
+    k_hooks_pick<H><<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(h, g->n);
+    k_hooks_prop<H><<<(unsigned)std::min<int64_t>(cdiv(g->n, 4), 148 * 64), 128, 0, c.s>>>(
+        h, g->n, g->d_hook_keys, g->d_hook_vals, g->d_changed + step, g->d_err);
+    c.launches += 2;
+    GLP_CUDA(cudaGetLastError());
+    if ((rc = after_iter(c, step, h.st.Lnext))) return rc;
+  }
+  return GLP_OK;
+}
+
+static int run_hooks(RunCtx& c, const glp_params& p, int32_t niter) {
+  glp_graph* g = c.g;
+  if (g->max_degree > kHookSmemCap / 2 && !g->d_hook_keys) {
+    GLP_CUDA(cudaMalloc(&g->d_hook_keys, sizeof(uint32_t) * 2 * (size_t)g->m));
+    GLP_CUDA(cudaMalloc(&g->d_hook_vals, sizeof(double) * 2 * (size_t)g->m));
+  }
+  HookState st{g->d_off, g->d_cols, g->d_w, g->d_lab[0], g->d_lab[1], nullptr, nullptr, 1.0};
+  c.iter_base = 1;  // Lnext holds the final labels
+  int rc;
+  if (p.hooks == GLP_HOOKS_LAYERED) {
+    int64_t have0 = 0, have1 = 0;
+    if (!g->d_vol[0]) {
+      if ((rc = grow(&g->d_vol[0], &have0, g->n)) || (rc = grow(&g->d_vol[1], &have1, g->n))) return rc;
+    }
+    int32_t* vol_r = g->d_vol[0];
+    int32_t* vol_w = g->d_vol[1];
+    GLP_CUDA(cudaMemsetAsync(vol_r, 0, sizeof(int32_t) * g->n, c.s));
+    GLP_CUDA(cudaMemsetAsync(vol_w, 0, sizeof(int32_t) * g->n, c.s));
+    for (int32_t layer = 0; layer < p.nlayers; ++layer) {
+      if ((rc = init_labels(c))) return rc;
+      st.dstar = (double)p.dstar[layer];
+      if ((rc = hooks_iterations(c, HooksLayered{st}, niter, layer * niter, true, &vol_r, &vol_w))) return rc;
+    }
+    g->d_vol[0] = vol_r;
+    g->d_vol[1] = vol_w;
+    return GLP_OK;
+  }
+  if ((rc = init_labels(c))) return rc;
+  int32_t* vr = nullptr;
+  int32_t* vw = nullptr;
+  if (p.hooks == GLP_HOOKS_CLASSIC) return hooks_iterations(c, HooksClassic{st}, niter, 0, false, &vr, &vw);
+  return hooks_iterations(c, HooksWeightedDegree{st}, niter, 0, false, &vr, &vw);
+}
+
+}  // namespace glp
+
+using namespace glp;
+
+// ================================================================ C ABI
+extern "C" {
+
+const char* glp_last_error(void) { return g_err.c_str(); }
+const char* glp_version(void) { return "glp_b200 0.1 (sm_100a)"; }
+
+int glp_params_default(glp_params* p) {
+  if (!p) {
+    set_error("params is NULL");
+    return GLP_EINVAL;
+  }
+  std::memset(p, 0, sizeof *p);
+  p->struct_size = (int32_t)sizeof(glp_params);
+  p->backend = GLP_BACKEND_EXACT;
+  // gamma in {1, 1/2, 1/4, 1/8, 1/16} -> dstar = 1/gamma + 1
+  p->nlayers = 5;
+  const int32_t ds[5] = {2, 3, 5, 9, 17};
+  for (int i = 0; i < 5; ++i) p->dstar[i] = ds[i];
+  p->slpa_T = 20;
+  p->slpa_r = 0.1;
+  p->seed = 4;
+  p->hooks = GLP_HOOKS_CLASSIC;
+  p->use_graph = 0;
+  p->async = 0;
+  return GLP_OK;
+}
+
+int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n, int64_t m,
+                     int32_t on_device, glp_graph** out) {
+  if (!out) {
+    set_error("out is NULL");
+    return GLP_EINVAL;
+  }
+  *out = nullptr;
+  if (n < 0 || m < 0 || m > INT32_MAX || !offsets || (m > 0 && !cols)) {
+    set_error("bad graph arguments (n=%d, m=%lld)", n, (long long)m);
+    return GLP_EINVAL;
+  }
+  int rc = require_device();
+  if (rc) return rc;
+  std::unique_ptr<glp_graph> g(new glp_graph());
+  g->n = n;
+  g->m = m;
+  GLP_CUDA(cudaGetDevice(&g->device));
+  g->h_off.resize((size_t)n + 1);
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (on_device)
+    GLP_CUDA(cudaMemcpy(g->h_off.data(), offsets, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost));
+  else
+    std::memcpy(g->h_off.data(), offsets, sizeof(int32_t) * ((size_t)n + 1));
+  // validate offsets on the host (they are needed there for planning anyway)
+  if (g->h_off[0] != 0 || (int64_t)g->h_off[n] != m) {
+    set_error("offsets[0]=%d, offsets[n]=%d, m=%lld", g->h_off[0], g->h_off[n], (long long)m);
+    return GLP_EINVAL;
+  }
+  int32_t maxd = 0;
+  for (int32_t v = 0; v < n; ++v) {
+    const int32_t d = g->h_off[v + 1] - g->h_off[v];
+    if (d < 0) {
+      set_error("offsets not monotone at vertex %d", v);
+      return GLP_EINVAL;
+    }
+    maxd = std::max(maxd, d);
+  }
+  g->max_degree = maxd;
+  GLP_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  GLP_CUDA(cudaMalloc(&g->d_off, sizeof(int32_t) * ((size_t)n + 1)));
+  GLP_CUDA(cudaMemcpy(g->d_off, g->h_off.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice));
+  GLP_CUDA(cudaMalloc(&g->d_cols, sizeof(int32_t) * std::max<int64_t>(m, 1)));
+  if (m) GLP_CUDA(cudaMemcpy(g->d_cols, cols, sizeof(int32_t) * m, kind));
+  if (weights) {
+    GLP_CUDA(cudaMalloc(&g->d_w, sizeof(int32_t) * std::max<int64_t>(m, 1)));
+    if (m) GLP_CUDA(cudaMemcpy(g->d_w, weights, sizeof(int32_t) * m, kind));
+  }
+  // validate columns (and weights) on the device
+  if ((rc = validate_csr_device(g.get()))) return rc;
+  *out = g.release();
+  return GLP_OK;
+}
+
+void glp_graph_destroy(glp_graph* g) {
+  if (!g) return;
+  free_plan(&g->plan);
+  cudaFree(g->d_off);
+  cudaFree(g->d_cols);
+  cudaFree(g->d_w);
+  cudaFree(g->d_lab[0]);
+  cudaFree(g->d_lab[1]);
+  cudaFree(g->d_vol[0]);
+  cudaFree(g->d_vol[1]);
+  cudaFree(g->d_spoken);
+  cudaFree(g->d_mem);
+  cudaFree(g->d_changed);
+  cudaFree(g->d_err);
+  cudaFree(g->d_hook_keys);
+  cudaFree(g->d_hook_vals);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+int glp_graph_info(const glp_graph* g, int32_t* n, int64_t* m, int32_t* max_degree) {
+  if (!g) {
+    set_error("graph is NULL");
+    return GLP_EINVAL;
+  }
+  if (n) *n = g->n;
+  if (m) *m = g->m;
+  if (max_degree) *max_degree = g->max_degree;
+  return GLP_OK;
+}
+
+int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int64_t out[16]) {
+  if (!offsets || !out || n < 0) {
+    set_error("NULL argument or n < 0");
+    return GLP_EINVAL;
+  }
+  for (int32_t v = 0; v < n; ++v)
+    if (offsets[v + 1] < offsets[v]) {
+      set_error("offsets not monotone at vertex %d", v);
+      return GLP_EINVAL;
+    }
+  TierParams t;
+  int rc = resolve_tiers(p, &t);
+  if (rc) return rc;
+  HostPlan hp;
+  build_host_plan(offsets, n, t, &hp);
+  auto edges = [&](const std::vector<int32_t>& vs) {
+    int64_t e = 0;
+    for (int32_t v : vs) e += offsets[v + 1] - offsets[v];
+    return e;
+  };
+  out[0] = hp.isolated;
+  out[1] = (int64_t)hp.tiny.size();
+  out[2] = (int64_t)hp.g16.size();
+  out[3] = (int64_t)hp.g32.size();
+  out[4] = (int64_t)hp.mid.size();
+  out[5] = (int64_t)hp.big.size();
+  out[6] = (int64_t)hp.hub_v.size();
+  out[7] = (int64_t)hp.chunk_hub.size();
+  out[8] = 0;
+  out[9] = edges(hp.tiny);
+  out[10] = edges(hp.g16);
+  out[11] = edges(hp.g32);
+  out[12] = edges(hp.mid);
+  out[13] = edges(hp.big);
+  out[14] = edges(hp.hub_v);
+  out[15] = hp.table_slots;
+  return GLP_OK;
+}
+
+int glp_graph_plan(glp_graph* g, const glp_params* p, int64_t out[16]) {
+  if (!g) {
+    set_error("graph is NULL");
+    return GLP_EINVAL;
+  }
+  return glp_plan_offsets(g->h_off.data(), g->n, p, out);
+}
+
+int glp_graph_check(glp_graph* g) {
+  if (!g) {
+    set_error("graph is NULL");
+    return GLP_EINVAL;
+  }
+  if (!g->d_err) return GLP_OK;
+  return check_err(g, g->stream);
+}
+
+int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, glp_outputs* out, glp_iter_cb cb,
+            void* cb_user, void* stream) {
+  if (!g || !out || !out->labels) {
+    set_error("graph, outputs and outputs->labels are required");
+    return GLP_EINVAL;
+  }
+  if (niter < 0) {
+    set_error("niter %d < 0", niter);
+    return GLP_EINVAL;
+  }
+  glp_params p;
+  glp_params_default(&p);
+  if (pin) {
+    if (pin->struct_size != (int32_t)sizeof(glp_params)) {
+      set_error("glp_params.struct_size %d != %d", pin->struct_size, (int)sizeof(glp_params));
+      return GLP_EINVAL;
+    }
+    p = *pin;
+  }
+  if (p.async && (cb || !out->on_device || out->changed || out->tier_ms || out->slpa_comm || out->slpa_mem)) {
+    set_error("async runs take device outputs only (labels/vol), no callback, no host-side reports");
+    return GLP_EINVAL;
+  }
+  int32_t total = niter;
+  switch (method) {
+    case GLP_METHOD_CLASSIC:
+      break;
+    case GLP_METHOD_LAYERED:
+      if (p.nlayers < 1 || p.nlayers > GLP_MAX_LAYERS) {
+        set_error("nlayers %d outside [1, %d]", p.nlayers, GLP_MAX_LAYERS);
+        return GLP_EINVAL;
+      }
+      for (int i = 0; i < p.nlayers; ++i)
+        if (p.dstar[i] < 1 || p.dstar[i] > 65536) {
+          set_error("dstar[%d] = %d outside [1, 65536]", i, p.dstar[i]);
+          return GLP_EINVAL;
+        }
+      total = p.nlayers * niter;
+      break;
+    case GLP_METHOD_SLPA:
+      if (p.slpa_T < 1 || p.slpa_T > 64) {
+        set_error("slpa_T %d outside [1, 64]", p.slpa_T);
+        return GLP_EINVAL;
+      }
+      if (!(p.slpa_r >= 0.0 && p.slpa_r <= 1.0)) {
+        set_error("slpa_r outside [0, 1]");
+        return GLP_EINVAL;
+      }
+      break;
+    case GLP_METHOD_USER:
+      if (p.hooks < GLP_HOOKS_CLASSIC || p.hooks > GLP_HOOKS_WEIGHTED_DEGREE) {
+        set_error("unknown hook set %d", p.hooks);
+        return GLP_EINVAL;
+      }
+      if (p.hooks == GLP_HOOKS_LAYERED) total = p.nlayers * niter;
+      break;
+    default:
+      set_error("method %d not in 1..4", method);
+      return GLP_ENOTSUP;
+  }
+  if (p.backend != GLP_BACKEND_EXACT && p.backend != GLP_BACKEND_CM && p.backend != GLP_BACKEND_FA) {
+    set_error("unknown backend %d", p.backend);
+    return GLP_EINVAL;
+  }
+  TierParams t;
+  int rc = resolve_tiers(&p, &t);
+  if (rc) return rc;
+  if (g->n == 0) {
+    if (out->changed)
+      for (int32_t i = 0; i < total; ++i) out->changed[i] = 0;
+    if (out->launches) *out->launches = 0;
+    return GLP_OK;
+  }
+  GLP_CUDA(cudaSetDevice(g->device));
+  if ((rc = ensure_plan(g, t))) return rc;
+  if ((rc = ensure_work(g, total))) return rc;
+  RunCtx c;
+  c.g = g;
+  c.s = stream ? (cudaStream_t)stream : g->stream;
+  c.cb = cb;
+  c.user = cb_user;
+  c.timing = out->tier_ms != nullptr;
+  GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
+  const bool W = g->d_w != nullptr;
+  switch (method) {
+    case GLP_METHOD_CLASSIC:
+      rc = W ? run_classic<true>(c, niter) : run_classic<false>(c, niter);
+      c.iter_base = niter & 1;
+      break;
+    case GLP_METHOD_LAYERED:
+      rc = W ? run_layered<true>(c, p, niter) : run_layered<false>(c, p, niter);
+      break;
+    case GLP_METHOD_SLPA:
+      rc = W ? run_slpa<true>(c, p, niter, out) : run_slpa<false>(c, p, niter, out);
+      c.iter_base = niter & 1;
+      break;
+    case GLP_METHOD_USER:
+      rc = run_hooks(c, p, niter);
+      break;
+  }
+  if (rc) return rc;
+  const int32_t* final_lab = g->d_lab[c.iter_base];
+  if (g->n)
+    GLP_CUDA(cudaMemcpyAsync(out->labels, final_lab, sizeof(int32_t) * g->n,
+                             out->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.s));
+  if (out->vol && g->n && (method == GLP_METHOD_LAYERED || (method == GLP_METHOD_USER && p.hooks == GLP_HOOKS_LAYERED)))
+    GLP_CUDA(cudaMemcpyAsync(out->vol, g->d_vol[1], sizeof(int32_t) * g->n,
+                             out->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.s));
+  if (out->launches) *out->launches = c.launches;
+  if (p.async) return GLP_OK;
+  if (out->changed && total > 0) {
+    std::vector<unsigned long long> tmp(total);
+    GLP_CUDA(cudaMemcpyAsync(tmp.data(), g->d_changed, sizeof(unsigned long long) * total, cudaMemcpyDeviceToHost,
+                             c.s));
+    GLP_CUDA(cudaStreamSynchronize(c.s));
+    for (int32_t i = 0; i < total; ++i) out->changed[i] = (int64_t)tmp[i];
+  }
+  if (out->tier_ms) {
+    if ((rc = c.harvest())) return rc;
+    for (int i = 0; i < 8; ++i) out->tier_ms[i] = c.tier_ms[i];
+  }
+  return check_err(g, c.s);
+}
+
+void glp_free_host(void* p) { std::free(p); }
+
+}  // extern "C"

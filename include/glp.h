@@ -1,0 +1,182 @@
+/*
+ * glp.h -- C ABI of the B200 label-propagation engine (libglp_b200.so).
+ *
+ * The reference (Gibyeng/GLP) has no C ABI: its surface is header-only C++
+ * templates.  Each entry point below names the reference interface it
+ * replaces, so a binding for any FFI (ctypes, cgo, JNI, N-API) can be written
+ * against plain pointers and sizes.
+ *
+ * Conventions
+ *   - Every call returns 0 on success or a negative GLP_E* code; no exception
+ *     crosses the ABI.  glp_last_error() gives the message of the calling
+ *     thread's last failure.
+ *   - Vertex ids and labels are int32; the CSR has n+1 int32 offsets and m
+ *     int32 column indices (m < 2^31), exactly the reference's
+ *     CSRGraph<int32_t,int32_t> layout (header/graph.h:61-198).
+ *   - A handle is thread-compatible, not thread-safe: one thread at a time.
+ *   - Streams are passed as void* (a cudaStream_t); NULL means the engine's
+ *     own stream for that handle.
+ *   - There is no CPU fallback: without a usable CUDA device every compute
+ *     call fails with GLP_ENODEV.
+ */
+#ifndef GLP_B200_GLP_H
+#define GLP_B200_GLP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GLP_OK 0
+#define GLP_EINVAL (-1)   /* bad argument or malformed CSR */
+#define GLP_ENOMEM (-2)   /* device or host allocation failed, or over budget */
+#define GLP_ECUDA (-3)    /* a CUDA call failed */
+#define GLP_ENOTSUP (-4)  /* method / option not supported */
+#define GLP_ENODEV (-5)   /* no usable CUDA device */
+#define GLP_ETIMEOUT (-6) /* a bounded wait ran out */
+#define GLP_ECANCELED (-7)/* request cancelled */
+#define GLP_EKERNEL (-8)  /* a kernel reported an internal error flag */
+#define GLP_EAGAIN (-9)   /* nothing ready yet (server poll) */
+
+/* ---- methods (main.cu:63-101 switch) ----------------------------------- */
+#define GLP_METHOD_CLASSIC 1 /* prop/classicLprop.cuh */
+#define GLP_METHOD_LAYERED 2 /* prop/MultiLprop.cuh + tutorial/CPUlp.cuh:169-262 */
+#define GLP_METHOD_SLPA 3    /* prop/SLPAprop.cuh, semantics tutorial/Base5prop.cuh */
+#define GLP_METHOD_USER 4    /* prop/UserdefinedLprop.cuh + README.md:72-101 hooks */
+
+/* ---- counting back-ends (method/hashtable.cuh, countmin.cuh, frequent.cuh) */
+#define GLP_BACKEND_EXACT 0 /* shared/global hash tables (GlobalHT) */
+#define GLP_BACKEND_CM 1    /* count-min sketch screen + exact fallback */
+#define GLP_BACKEND_FA 2    /* Misra-Gries frequent table screen + exact fallback */
+
+/* ---- built-in hook sets for method 4 ----------------------------------- */
+#define GLP_HOOKS_CLASSIC 0 /* README.md:83-101 example: (L[sid], 1), score = freq */
+#define GLP_HOOKS_LAYERED 1 /* score = dstar*freq - vol[l], UpdateVertex counts vol */
+#define GLP_HOOKS_WEIGHTED_DEGREE 2 /* freq = w / deg(sid) in FP64 (non-monotone score demo) */
+
+#define GLP_MAX_LAYERS 32
+
+typedef struct glp_graph glp_graph;
+
+/* Parameters.  glp_params_default() fills every field; callers then change
+ * what they need.  Replaces the constants hard-coded in the reference's
+ * perform_lp (prop/classicLprop.cuh:176-198, :381; prop/MultiLprop.cuh:148;
+ * prop/SLPAprop.cuh:31). */
+typedef struct glp_params {
+  int32_t struct_size;            /* = sizeof(glp_params) */
+  int32_t backend;                /* GLP_BACKEND_* */
+  /* layered LP: layer s uses the integer score dstar[s]*k - vol[l], which
+   * orders labels exactly as k - gamma*(vol-k) with gamma = 1/(dstar-1). */
+  int32_t nlayers;
+  int32_t dstar[GLP_MAX_LAYERS];
+  /* SLPA */
+  int32_t slpa_T;                 /* memory slots per vertex (1..64) */
+  double slpa_r;                  /* post-processing threshold */
+  uint64_t seed;                  /* speaker hash seed */
+  /* method 4 */
+  int32_t hooks;                  /* GLP_HOOKS_* */
+  /* degree tiers (0 = engine default / autotuned) */
+  int32_t tiny_max;               /* thread per vertex up to this degree */
+  int32_t mid_max;                /* warp per vertex up to this degree */
+  int32_t big_max;                /* block per vertex up to this degree; above: hub chunks */
+  int32_t hub_chunk;              /* edges per hub block */
+  int32_t use_graph;              /* capture the iteration loop in a CUDA graph */
+  int32_t async;                  /* 1: enqueue on the stream and return without
+                                     synchronising (device outputs only, no
+                                     callback); kernel error flags are then
+                                     reported by glp_graph_check() */
+  int32_t reserved[8];
+} glp_params;
+
+/* Per-iteration observer (parity checks).  labels is a HOST copy of the
+ * labels after iteration `iter` (0-based; layered: layer*niter + iter).
+ * Return non-zero to stop the run early (status GLP_ECANCELED). */
+typedef int (*glp_iter_cb)(int32_t iter, const int32_t* labels, int32_t n, void* user);
+
+/* Outputs of glp_run.  labels is required; the others are optional. */
+typedef struct glp_outputs {
+  int32_t* labels;      /* [n] final labels */
+  int32_t* slpa_comm;   /* [n][slpa_T] communities kept by post-processing, ascending, -1 padded */
+  int32_t* slpa_ncomm;  /* [n] number of communities kept */
+  int32_t* slpa_mem;    /* [slpa_T][n] speaker memory, -1 = empty */
+  int32_t* vol;         /* [n] layered: label volumes after the last iteration */
+  int64_t* changed;     /* [iterations] labels changed per iteration (host) */
+  float* tier_ms;       /* [8] host: summed device ms per kernel tier (tiny, group16,
+                           group32, mid, big, hub, aux, -), timed with CUDA events
+                           on the run's stream; NULL = no per-tier events */
+  int64_t* launches;    /* [1] host: kernels this run launched */
+  int32_t on_device;    /* 1: labels/slpa/vol pointers are device pointers */
+} glp_outputs;
+
+const char* glp_last_error(void);
+const char* glp_version(void);
+int glp_params_default(glp_params* p);
+
+/* Graph handle.  Replaces CSRGraph + the propagator's preprocess()
+ * (header/graph.h:61-198, prop/classicLprop.cuh:65-78): the CSR is copied
+ * to (or adopted on) the device once and stays resident across runs.
+ * weights may be NULL; non-NULL weights must be >= 0 (integer edge weights,
+ * summed exactly).  on_device = 1: the pointers are device pointers
+ * (copied device-to-device).  The CSR is validated (monotone offsets, columns
+ * in [0,n)); a malformed CSR returns GLP_EINVAL. */
+int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n,
+                     int64_t m, int32_t on_device, glp_graph** out);
+void glp_graph_destroy(glp_graph* g);
+int glp_graph_info(const glp_graph* g, int32_t* n, int64_t* m, int32_t* max_degree);
+/* Degree-tier plan for these params.  out[0..6]: vertices per tier
+ * [isolated, tiny, group16, group32, mid, big, hub]; out[7]: hub blocks;
+ * out[8..14]: CSR entries (edges) per tier in the same order; out[15]:
+ * global hub-table slots.  Mirrors the bin report of
+ * prop/classicLprop.cuh:213-227. */
+int glp_graph_plan(glp_graph* g, const glp_params* p, int64_t out[16]);
+/* The same plan computed from host offsets alone (no device needed). */
+int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int64_t out[16]);
+/* Reports (and clears) kernel error flags raised by asynchronous runs. */
+int glp_graph_check(glp_graph* g);
+
+/* Run `method` for niter iterations (layered: nlayers*niter).  Replaces
+ * XProp<V,E>::run(niter) of prop/classicLprop.cuh:454-462,
+ * prop/MultiLprop.cuh:384-392, prop/SLPAprop.cuh and
+ * prop/UserdefinedLprop.cuh, selected as main.cu:63-101 does.  Labels start
+ * at the vertex id (kernel.cuh:444-451).  Unlike the reference, labels are
+ * returned.  The call is synchronous with respect to the host. */
+int glp_run(glp_graph* g, int32_t method, const glp_params* p, int32_t niter, glp_outputs* out,
+            glp_iter_cb cb, void* cb_user, void* stream);
+
+/* ---- synthetic graph samplers (input synthesis for tests and benchmarks) --
+ * Deterministic counter-based sampling: sample i depends only on (seed, i),
+ * so host and device produce identical edge lists.  on_device selects where
+ * src/dst live.  R-MAT quadrant probabilities a,b,c (d = 1-a-b-c). */
+int glp_sample_rmat(int32_t scale, double a, double b, double c, uint64_t seed, int64_t first, int64_t count,
+                    int32_t* src, int32_t* dst, int32_t on_device);
+/* Planted partition: n vertices in k equal communities (community of v =
+ * v / ceil(n/k)); samples [0, n_intra) are intra-community, the rest are
+ * inter-community. */
+int glp_sample_planted(int32_t n, int32_t k, int64_t n_intra, uint64_t seed, int64_t first, int64_t count,
+                       int32_t* src, int32_t* dst, int32_t on_device);
+/* Overlapping planted partition (SLPA workload): every vertex is in its home
+ * community v / ceil(n/k); a fraction `overlap` of vertices (chosen by hash)
+ * also belongs to a second community.  An edge picks u, one of u's
+ * communities, and a uniform member of it. */
+int glp_sample_overlap(int32_t n, int32_t k, double overlap, uint64_t seed, int64_t first, int64_t count,
+                       int32_t* src, int32_t* dst, int32_t on_device);
+/* Edge weight w = 1 + (H(seed, min(u,v), max(u,v)) mod wmax): symmetric. */
+int glp_edge_weights(const int32_t* off, const int32_t* cols, int32_t n, int64_t m, int32_t wmax, uint64_t seed,
+                     int32_t* w, int32_t on_device);
+
+/* ---- reference-format graph I/O (tools/ + header/graph.h) ---------------
+ * Load a binary int32 (u,v) pair file with the semantics of
+ * load_edgelist_bin + CSRGraph (header/graph.h:69-147, :226-258): self
+ * loops dropped, symmetrised unless direct, duplicates kept, neighbour order
+ * = file order, n = max id + 1.  Returns host buffers owned by the library
+ * (free with glp_free_host). */
+int glp_load_edgelist_bin(const char* path, int32_t direct, int32_t** offsets, int32_t** cols, int32_t* n,
+                          int64_t* m);
+void glp_free_host(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLP_B200_GLP_H */

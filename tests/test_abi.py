@@ -1,0 +1,89 @@
+"""The C ABI library loads, exports every declared entry point, validates
+arguments, and fails loudly (no CPU fallback) when there is no GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from glp_b200 import _lib
+from glp_b200.engine import make_params
+
+HEADERS = [os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", h) for h in ("glp.h",)]
+
+
+def declared_symbols():
+    names = set()
+    for h in HEADERS:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        names |= set(re.findall(r"\b(glp_[a-z0-9_]+)\s*\(", txt))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported():
+    lib = _lib.load()
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) <= set(_lib.SIGNATURES) | set(_lib.OPTIONAL_SIGNATURES)
+
+
+def test_params_defaults():
+    p = _lib.default_params()
+    assert p.struct_size == C.sizeof(_lib.Params)
+    assert p.nlayers == 5 and list(p.dstar[:5]) == [2, 3, 5, 9, 17]
+    assert p.slpa_T == 20 and abs(p.slpa_r - 0.1) < 1e-12
+    q = make_params(gammas=[1, 0.5, 0.25])
+    assert list(q.dstar[:3]) == [2, 3, 5] and q.nlayers == 3
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU path")
+def test_no_gpu_fails_loudly():
+    from glp_b200.engine import Graph
+    from glp_b200.graphs import from_numpy
+    g = from_numpy(np.array([0, 1, 2], np.int32), np.array([1, 0], np.int32))
+    with pytest.raises(_lib.GlpError) as e:
+        Graph(g)
+    assert e.value.code == _lib.GLP_ENODEV
+
+
+def _plan(off, **kw):
+    lib = _lib.load()
+    out = (C.c_int64 * 16)()
+    p = make_params(**kw)
+    off = np.ascontiguousarray(off, np.int32)
+    rc = lib.glp_plan_offsets(off.ctypes.data_as(C.c_void_p), len(off) - 1, C.byref(p), out)
+    return rc, list(out)
+
+
+def test_planner_tiers():
+    degs = [0, 1, 8, 9, 16, 17, 32, 33, 256, 257, 4096, 4097, 10000]
+    off = np.concatenate([[0], np.cumsum(degs)]).astype(np.int32)
+    rc, out = _plan(off)
+    assert rc == 0
+    assert out[:7] == [1, 2, 2, 2, 2, 2, 2]  # isolated, tiny, g16, g32, mid, big, hub
+    assert out[7] == 2 + 3  # hub blocks: ceil(4097/4096) + ceil(10000/4096)
+    assert out[9] == 9 and out[14] == 4097 + 10000
+    rc, out = _plan(off, tiny_max=4, mid_max=64, big_max=512, hub_chunk=256)
+    assert rc == 0 and out[1] == 1 and out[2] == 3 and out[5] == 2 and out[6] == 3
+
+
+def test_planner_rejects_bad_input():
+    rc, _ = _plan(np.array([0, 5, 3], np.int32))
+    assert rc == _lib.GLP_EINVAL
+    rc, _ = _plan(np.array([0, 1], np.int32), tiny_max=9)
+    assert rc == _lib.GLP_EINVAL
+    rc, _ = _plan(np.array([0, 1], np.int32), mid_max=300)
+    assert rc == _lib.GLP_EINVAL
+
+
+def test_bad_method_and_null_args():
+    lib = _lib.load()
+    out = _lib.Outputs()
+    rc = lib.glp_run(None, 1, None, 1, C.byref(out), _lib.ITER_CB(), None, None)
+    assert rc == _lib.GLP_EINVAL
+    assert b"required" in lib.glp_last_error()

@@ -1,0 +1,257 @@
+"""Bit-exact parity of the CUDA engine with the CPU oracle.
+
+Every case runs through the C ABI (glp_run via glp_b200.engine.Graph) and is
+compared with the oracle after EVERY iteration: integer labels must be equal,
+no tolerance.  Tier parameter sets shrink the degree thresholds so that small
+graphs drive every kernel (tiny, group16/32, mid, big, multi-chunk hub).
+"""
+import numpy as np
+import pytest
+
+from glp_b200 import _lib
+from glp_b200.engine import Graph, make_params
+from glp_b200.graphs import from_numpy
+from oracle import oracle as O
+from tests.graphs_fixtures import (BOUNDARY_DEGREES, cycle, degree_ladder, path, planted_np, rmat_np, star,
+                                   two_cliques, undirected)
+
+pytestmark = pytest.mark.gpu
+
+
+def _star_ring(leaves):
+    e = [(0, i) for i in range(1, leaves + 1)] + [(i, i % leaves + 1) for i in range(1, leaves + 1)]
+    return undirected(leaves + 1, e)
+
+
+def _cases():
+    cases = {
+        "path": path(50),
+        "cycle": cycle(31),
+        "star": star(100),
+        "star_ring_3000": _star_ring(3000),
+        "two_cliques": two_cliques(20),
+        "ladder": degree_ladder(BOUNDARY_DEGREES),
+        "isolated_only": (np.zeros(6, np.int32), np.zeros(0, np.int32)),
+    }
+    off, cols, _ = rmat_np(12, seed=1)
+    cases["rmat12"] = (off, cols)
+    off, cols, _ = rmat_np(14, seed=2)
+    cases["rmat14"] = (off, cols)
+    off, cols, _ = planted_np(20000, 40, 18.0, 2.0, 3)
+    cases["planted20k"] = (off, cols)
+    return cases
+
+
+CASES = _cases()
+TIERS = {
+    "default": {},
+    "small_hubs": dict(tiny_max=4, mid_max=64, big_max=128, hub_chunk=256),
+    "no_tiny": dict(tiny_max=-1, mid_max=32, big_max=32, hub_chunk=512),
+}
+
+
+def _run_trace(off, cols, method, niter, w=None, **kw):
+    g = Graph(from_numpy(off, cols, w))
+    trace = []
+    res = g.run(method, niter, make_params(**kw), callback=lambda it, lab: trace.append(lab) and False)
+    g.close()
+    return res, np.array(trace).reshape(-1, len(off) - 1)
+
+
+@pytest.mark.parametrize("tier", list(TIERS))
+@pytest.mark.parametrize("case", list(CASES))
+def test_classic_per_iteration(case, tier):
+    off, cols = CASES[case]
+    niter = 8
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, niter, **TIERS[tier])
+    _, otr = O.classic_run(off, cols, niter, trace=True)
+    for it in range(niter):
+        np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
+    np.testing.assert_array_equal(res.labels, otr[-1])
+    prev = np.arange(len(off) - 1)
+    for it in range(niter):
+        assert res.changed[it] == int((otr[it] != prev).sum())
+        prev = otr[it]
+
+
+@pytest.mark.parametrize("tier", ["default", "small_hubs"])
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "planted20k"])
+def test_weighted_per_iteration(case, tier):
+    off, cols = CASES[case]
+    w = (np.arange(len(cols), dtype=np.int64) * 2654435761 % 16 + 1).astype(np.int32)
+    # symmetric weights are not required by the rule; use the engine's symmetric ones for realism
+    from glp_b200 import graphs
+    w = graphs.add_weights(from_numpy(off, cols), 16, seed=7).weights.numpy()
+    niter = 6
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, niter, w=w, **TIERS[tier])
+    _, otr = O.classic_run(off, cols, niter, w=w, trace=True)
+    for it in range(niter):
+        np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
+
+
+@pytest.mark.parametrize("tier", ["default", "small_hubs"])
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "two_cliques", "planted20k"])
+def test_layered_per_iteration(case, tier):
+    off, cols = CASES[case]
+    dstar = [2, 3, 5, 9, 17]
+    niter = 3
+    res, tr = _run_trace(off, cols, _lib.METHOD_LAYERED, niter, dstar=dstar, **TIERS[tier])
+    lab, vol, otr = O.layered_run(off, cols, dstar, niter, trace=True)
+    for s in range(len(dstar) * niter):
+        np.testing.assert_array_equal(tr[s], otr[s], err_msg=f"step {s}")
+    np.testing.assert_array_equal(res.labels, lab)
+    np.testing.assert_array_equal(res.vol, vol)
+
+
+def test_layered_weighted():
+    off, cols = CASES["rmat12"]
+    from glp_b200 import graphs
+    w = graphs.add_weights(from_numpy(off, cols), 16, seed=3).weights.numpy()
+    res, tr = _run_trace(off, cols, _lib.METHOD_LAYERED, 3, w=w, dstar=[2, 17])
+    lab, vol, otr = O.layered_run(off, cols, [2, 17], 3, w=w, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+    np.testing.assert_array_equal(res.vol, vol)
+
+
+@pytest.mark.parametrize("tier", ["default", "small_hubs"])
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "planted20k", "path"])
+def test_slpa(case, tier):
+    off, cols = CASES[case]
+    T, niter, seed, r = 20, 20, 4, 0.1
+    g = Graph(from_numpy(off, cols))
+    trace = []
+    res = g.run(_lib.METHOD_SLPA, niter, make_params(slpa_T=T, seed=seed, slpa_r=r, **TIERS[tier]),
+                callback=lambda it, lab: trace.append(lab) and False, slpa_outputs=True)
+    g.close()
+    ref = O.slpa_run(off, cols, T, niter, seed, r)
+    np.testing.assert_array_equal(res.labels, ref["labels"])
+    np.testing.assert_array_equal(res.slpa_mem, ref["mem"])
+    np.testing.assert_array_equal(res.slpa_comm, ref["comm"])
+    np.testing.assert_array_equal(res.slpa_ncomm, ref["ncomm"])
+
+
+@pytest.mark.parametrize("T,niter", [(1, 5), (5, 3), (5, 12), (64, 10)])
+def test_slpa_memory_sizes(T, niter):
+    off, cols = CASES["rmat12"]
+    g = Graph(from_numpy(off, cols))
+    res = g.run(_lib.METHOD_SLPA, niter, make_params(slpa_T=T, seed=99, slpa_r=0.25), slpa_outputs=True)
+    g.close()
+    ref = O.slpa_run(off, cols, T, niter, 99, 0.25)
+    np.testing.assert_array_equal(res.labels, ref["labels"])
+    np.testing.assert_array_equal(res.slpa_mem, ref["mem"])
+    np.testing.assert_array_equal(res.slpa_comm, ref["comm"])
+
+
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000"])
+def test_hooks_classic_equals_method1(case):
+    off, cols = CASES[case]
+    res, tr = _run_trace(off, cols, _lib.METHOD_USER, 6, hooks=_lib.HOOKS_CLASSIC)
+    _, otr = O.classic_run(off, cols, 6, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+
+
+@pytest.mark.parametrize("case", ["rmat12", "star_ring_3000"])
+def test_hooks_layered_equals_method2(case):
+    off, cols = CASES[case]
+    res, tr = _run_trace(off, cols, _lib.METHOD_USER, 3, hooks=_lib.HOOKS_LAYERED, dstar=[2, 5, 17])
+    lab, vol, otr = O.layered_run(off, cols, [2, 5, 17], 3, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+    np.testing.assert_array_equal(res.vol, vol)
+
+
+def _weighted_degree_reference(off, cols, niter):
+    """FP64 degree-normalised frequencies summed in the engine's documented
+    order: within each 32-edge chunk in lane order, chunks in CSR order."""
+    n = len(off) - 1
+    deg = np.diff(off).astype(np.float64)
+    lab = np.arange(n, dtype=np.int64)
+    for _ in range(niter):
+        new = lab.copy()
+        for v in range(n):
+            b, e = off[v], off[v + 1]
+            if b == e:
+                continue
+            acc = {}
+            for c0 in range(b, e, 32):
+                chunk = {}
+                for j in range(c0, min(c0 + 32, e)):
+                    u = cols[j]
+                    chunk[lab[u]] = chunk.get(lab[u], 0.0) + 1.0 / deg[u]
+                for l, s in chunk.items():
+                    acc[l] = acc.get(l, 0.0) + s
+            new[v] = max(acc.items(), key=lambda kv: (kv[1], kv[0]))[0]
+        lab = new
+    return lab
+
+
+def test_hooks_weighted_degree_fp64_deterministic():
+    off, cols = degree_ladder([3, 40, 300, 700])
+    res, tr = _run_trace(off, cols, _lib.METHOD_USER, 3, hooks=_lib.HOOKS_WEIGHTED_DEGREE)
+    np.testing.assert_array_equal(tr[-1], _weighted_degree_reference(off, cols, 3))
+
+
+def test_rmat16_classic_20_iterations():
+    """The R-MAT scale-16 workload (edge factor 16, seed 1), 20 iterations."""
+    off, cols, _ = rmat_np(16, seed=1)
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, 20)
+    _, otr = O.classic_run(off, cols, 20, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+
+
+def test_device_outputs_and_repeat_runs_are_identical():
+    import torch
+    off, cols, _ = rmat_np(13, seed=5)
+    g = Graph(from_numpy(off, cols))
+    out = torch.empty(len(off) - 1, dtype=torch.int32, device="cuda")
+    r1 = g.run(_lib.METHOD_CLASSIC, 10, labels_out=out)
+    a = out.cpu().numpy()
+    r2 = g.run(_lib.METHOD_CLASSIC, 10)
+    g.close()
+    np.testing.assert_array_equal(a, r2.labels)
+    np.testing.assert_array_equal(a, O.classic_run(off, cols, 10))
+    assert r1.launches > 0
+
+
+def test_device_resident_csr_input():
+    import torch
+    off, cols, _ = rmat_np(12, seed=9)
+    dg = from_numpy(off, cols).to("cuda")
+    g = Graph(dg)
+    res = g.run(_lib.METHOD_CLASSIC, 5)
+    g.close()
+    np.testing.assert_array_equal(res.labels, O.classic_run(off, cols, 5))
+
+
+def test_malformed_csr_rejected():
+    off = np.array([0, 2, 3], np.int32)
+    cols = np.array([1, 5, 0], np.int32)  # 5 is out of range
+    with pytest.raises(_lib.GlpError) as e:
+        Graph(from_numpy(off, cols))
+    assert e.value.code == _lib.GLP_EINVAL
+    with pytest.raises(_lib.GlpError):
+        Graph(from_numpy(off, np.array([1, 1, 0], np.int32), np.array([1, -2, 1], np.int32)))
+
+
+def test_callback_can_stop_the_run():
+    off, cols = CASES["rmat12"]
+    g = Graph(from_numpy(off, cols))
+    with pytest.raises(_lib.GlpError) as e:
+        g.run(_lib.METHOD_CLASSIC, 10, callback=lambda it, lab: it == 2)
+    assert e.value.code == _lib.GLP_ECANCELED
+    res = g.run(_lib.METHOD_CLASSIC, 3)  # the handle stays usable
+    g.close()
+    np.testing.assert_array_equal(res.labels, O.classic_run(off, cols, 3))
+
+
+def test_generators_host_equal_device():
+    import torch
+    from glp_b200 import graphs
+    for fn, args in ((graphs.sample_rmat, (12, 16, 1)), (graphs.sample_planted, (5000, 10, 18.0, 2.0, 3)),
+                     (graphs.sample_overlap, (5000, 10, 0.1, 24.0, 4))):
+        a = fn(*args, device="cpu")
+        b = fn(*args, device="cuda")
+        assert torch.equal(a[0], b[0].cpu()) and torch.equal(a[1], b[1].cpu())
+    g1 = graphs.rmat(12, 16, seed=1, device="cpu", weighted=True)
+    g2 = graphs.rmat(12, 16, seed=1, device="cuda", weighted=True)
+    assert torch.equal(g1.offsets, g2.offsets.cpu()) and torch.equal(g1.cols, g2.cols.cpu())
+    assert torch.equal(g1.weights, g2.weights.cpu())
