@@ -44,8 +44,8 @@ import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
 ITERS = 20
-TIER_NAMES = ("tiny", "group16", "group32", "mid", "big", "hub", "aux", "-")
-TIER_PLAN_KEYS = ("tiny", "group16", "group32", "mid", "big", "hub")
+TIER_NAMES = ("tiny", "group16", "group32", "mid", "big", "hub", "aux", "majority")
+TIER_PLAN_KEYS = {0: "tiny", 1: "group16", 2: "group32", 3: "mid", 4: "big", 5: "hub"}
 
 
 def parse():
@@ -326,9 +326,9 @@ def run_glp(args, ws, rank, local):
     # roofline of the dominant kernel tier
     peak, peak_kind = measured_peak()
     launches_per_tier = args.steps * args.iters
-    dom = int(np.argmax(tier_ms[:6]))
+    dom = max(TIER_PLAN_KEYS, key=lambda i: tier_ms[i])
     key = TIER_PLAN_KEYS[dom]
-    n_t, m_t = plan[f"v_{key}"], plan[f"e_{key}"]
+    n_t, m_t = plan[f"v_{key}"], plan[f"e_{key}"]  # vertices and CSR entries of that kernel group
     bytes_launch = 8 * m_t + 12 * n_t
     avg_ms = tier_ms[dom] / launches_per_tier
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
@@ -373,7 +373,7 @@ def run_glp(args, ws, rank, local):
             "whole_step_roofline": {"bytes_per_iter": int(total_bytes_iter), "iter_ms": round(iter_ms, 4),
                                     "achieved_gbs": round(total_bytes_iter / (iter_ms / 1e3) / 1e9, 1),
                                     "frac": round(total_bytes_iter / (iter_ms / 1e3) / 1e9 / peak, 4)},
-            "tier_ms_per_iter": {TIER_NAMES[i]: round(tier_ms[i] / launches_per_tier, 4) for i in range(6)},
+            "tier_ms_per_iter": {TIER_NAMES[i]: round(tier_ms[i] / launches_per_tier, 4) for i in TIER_PLAN_KEYS},
             "plan": plan,
             "clocks": clk,
             "cpu_baseline": cpu,

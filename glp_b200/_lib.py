@@ -72,6 +72,8 @@ class Outputs(C.Structure):
         ("changed", C.c_void_p),
         ("tier_ms", C.c_void_p),
         ("launches", C.c_void_p),
+        ("iter_ms", C.c_void_p),
+        ("step_tier_ms", C.c_void_p),
         ("on_device", C.c_int32),
     ]
 

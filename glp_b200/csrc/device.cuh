@@ -113,10 +113,36 @@ struct CountTable {
   }
 };
 
-// Warp-aggregated increment of a counter.
-__device__ __forceinline__ void warp_count_add(unsigned long long* counter, bool flag) {
-  const uint32_t b = __ballot_sync(kFull, flag);
-  if ((threadIdx.x & 31) == 0 && b) atomicAdd(counter, (unsigned long long)__popc(b));
+// Bounded insert: gives up after `max_probe` probes and returns kNoSlot.
+// Optionally appends newly claimed slots to `claimed` (count in *nclaimed).
+constexpr uint32_t kNoSlot = 0xffffffffu;
+__device__ __forceinline__ uint32_t table_insert_bounded(uint32_t* keys, uint32_t* vals, uint32_t mask, uint32_t key,
+                                                         uint32_t c, uint32_t max_probe, uint32_t* claimed,
+                                                         uint32_t* nclaimed) {
+  uint32_t h = fmix32(key) & mask;
+  for (uint32_t probe = 0; probe < max_probe; ++probe) {
+    const uint32_t cur = keys[h];
+    if (cur == key) return atomicAdd(&vals[h], c) + c;
+    if (cur == 0) {
+      const uint32_t prev = atomicCAS(&keys[h], 0u, key);
+      if (prev == 0u) {
+        if (claimed) claimed[atomicAdd(nclaimed, 1u)] = h;
+        return atomicAdd(&vals[h], c) + c;
+      }
+      if (prev == key) return atomicAdd(&vals[h], c) + c;
+    }
+    h = (h + 1) & mask;
+  }
+  return kNoSlot;
+}
+
+// Smallest power of two >= x (x >= 1).
+__device__ __forceinline__ uint32_t pow2_ceil(uint32_t x) { return x <= 1 ? 1u : 1u << (32 - __clz(x - 1)); }
+
+// Warp-aggregated add of per-lane counts (0..255) to a counter.
+__device__ __forceinline__ void warp_count_add(unsigned long long* counter, uint32_t count) {
+  const uint32_t total = __reduce_add_sync(kFull, count);
+  if ((threadIdx.x & 31) == 0 && total) atomicAdd(counter, (unsigned long long)total);
 }
 
 }  // namespace glp

@@ -48,11 +48,6 @@ static int require_device() {
   return GLP_OK;
 }
 
-static uint64_t next_pow2(uint64_t x) {
-  uint64_t p = 1;
-  while (p < x) p <<= 1;
-  return p;
-}
 
 int resolve_tiers(const glp_params* p, TierParams* t) {
   TierParams d;
@@ -67,55 +62,68 @@ int resolve_tiers(const glp_params* p, TierParams* t) {
     set_error("tiny_max %d > 8", d.tiny_max);
     return GLP_EINVAL;
   }
-  if (d.mid_max < 32 || d.mid_max > 256) {
-    set_error("mid_max %d outside [32, 256]", d.mid_max);
+  if (d.mid_max < 32 || d.mid_max > kMidCap / 2) {
+    set_error("mid_max %d outside [32, %d]", d.mid_max, kMidCap / 2);
     return GLP_EINVAL;
   }
-  if (d.big_max < d.mid_max || d.big_max > 8192) {
-    set_error("big_max %d outside [mid_max, 8192]", d.big_max);
+  if (d.big_max < d.mid_max || d.big_max > kBigCap / 2) {
+    set_error("big_max %d outside [mid_max, %d]", d.big_max, kBigCap / 2);
     return GLP_EINVAL;
   }
-  if (d.hub_chunk < 256 || d.hub_chunk > 8192) {
-    set_error("hub_chunk %d outside [256, 8192]", d.hub_chunk);
+  if (d.hub_chunk < 256 || d.hub_chunk > 65536) {
+    set_error("hub_chunk %d outside [256, 65536]", d.hub_chunk);
     return GLP_EINVAL;
   }
   *t = d;
   return GLP_OK;
 }
 
+// Degree tiers; hubs get ceil(deg / kHubBucket) hash buckets (one work item
+// each) and streaming chunks of hub_chunk edges.
 void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPlan* hp) {
   *hp = HostPlan{};
   for (int32_t v = 0; v < n; ++v) {
     const int32_t d = off[v + 1] - off[v];
+    int tier;
     if (d == 0) {
       hp->isolated++;
+      tier = 0;
     } else if (d <= t.tiny_max) {
       hp->tiny.push_back(v);
+      tier = 1;
     } else if (d <= 16) {
       hp->g16.push_back(v);
+      tier = 2;
     } else if (d <= 32) {
       hp->g32.push_back(v);
+      tier = 3;
     } else if (d <= t.mid_max) {
       hp->mid.push_back(v);
+      hp->mb.push_back(v);
+      tier = 4;
     } else if (d <= t.big_max) {
       hp->big.push_back(v);
+      hp->mb.push_back(v);
+      tier = 5;
     } else {
+      tier = 6;
       const int32_t h = (int32_t)hp->hub_v.size();
-      const int32_t nch = (d + t.hub_chunk - 1) / t.hub_chunk;
+      const int32_t nb = (d + kHubBucket - 1) / kHubBucket;
       hp->hub_v.push_back(v);
-      hp->hub_nchunks.push_back(nch);
-      const uint64_t cap = next_pow2(2ull * (uint64_t)d);
-      hp->hub_tbase.push_back(hp->table_slots);
-      hp->hub_tmask.push_back((uint32_t)(cap - 1));
-      hp->table_slots += (int64_t)cap;
-      hp->hub_ubase.push_back(hp->used_slots);
-      hp->used_slots += d;
-      for (int32_t c = 0; c < nch; ++c) {
+      hp->hub_nb.push_back(nb);
+      hp->hub_lbase.push_back(hp->hub_labels);
+      hp->hub_labels += d;
+      for (int32_t b = 0; b < nb; ++b) {
+        hp->item_hub.push_back(h);
+        hp->item_bucket.push_back(b);
+      }
+      for (int64_t c = off[v]; c < off[v + 1]; c += t.hub_chunk) {
         hp->chunk_hub.push_back(h);
-        hp->chunk_begin.push_back(off[v] + c * t.hub_chunk);
-        hp->chunk_end.push_back(std::min(off[v + 1], off[v] + (c + 1) * t.hub_chunk));
+        hp->chunk_begin.push_back((int32_t)c);
+        hp->chunk_end.push_back((int32_t)std::min<int64_t>(off[v + 1], c + t.hub_chunk));
       }
     }
+    hp->edges[tier] += d;
   }
 }
 
@@ -134,6 +142,22 @@ static int upload(DevicePlan* p, const std::vector<T>& v, T** out) {
   GLP_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
   *out = static_cast<T*>(d);
   return GLP_OK;
+}
+
+// A tier whose vertex ids are consecutive becomes a range (no id list).
+static int upload_verts(DevicePlan* p, const std::vector<int32_t>& v, Verts* out) {
+  *out = Verts{nullptr, 0, (int32_t)v.size()};
+  if (v.empty()) return GLP_OK;
+  bool range = true;
+  for (size_t i = 1; i < v.size() && range; ++i) range = v[i] == v[0] + (int32_t)i;
+  if (range) {
+    out->base = v[0];
+    return GLP_OK;
+  }
+  int32_t* d = nullptr;
+  int rc = upload(p, v, &d);
+  out->ids = d;
+  return rc;
 }
 
 template <class T>
@@ -157,35 +181,34 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   p.tiers = t;
   p.isolated = hp.isolated;
   int rc;
-  if ((rc = upload(&p, hp.tiny, &p.tiny)) || (rc = upload(&p, hp.g16, &p.g16)) || (rc = upload(&p, hp.g32, &p.g32)) ||
-      (rc = upload(&p, hp.mid, &p.mid)) || (rc = upload(&p, hp.big, &p.big))) {
+  if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
+      (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
+      (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
+      (rc = zeroed(&p, 2, &p.fail_counts)) || (rc = zeroed(&p, std::max<size_t>(hp.mid.size(), 1), &p.fmid.ids)) ||
+      (rc = zeroed(&p, std::max<size_t>(hp.big.size(), 1), &p.fbig.ids))) {
     free_plan(&p);
     return rc;
   }
-  p.n_tiny = (int32_t)hp.tiny.size();
-  p.n_g16 = (int32_t)hp.g16.size();
-  p.n_g32 = (int32_t)hp.g32.size();
-  p.n_mid = (int32_t)hp.mid.size();
-  p.n_big = (int32_t)hp.big.size();
+  p.fmid.count = p.fail_counts;
+  p.fbig.count = p.fail_counts + 1;
   p.n_hubs = (int32_t)hp.hub_v.size();
   p.n_chunks = (int32_t)hp.chunk_hub.size();
-  p.big_cap = (uint32_t)next_pow2(2ull * (uint64_t)t.big_max);
-  p.hub_cap = (uint32_t)next_pow2(2ull * (uint64_t)t.hub_chunk);
   if (p.n_hubs) {
     HubPlan& h = p.hub;
     if ((rc = upload(&p, hp.chunk_hub, (int32_t**)&h.chunk_hub)) ||
         (rc = upload(&p, hp.chunk_begin, (int32_t**)&h.chunk_begin)) ||
         (rc = upload(&p, hp.chunk_end, (int32_t**)&h.chunk_end)) || (rc = upload(&p, hp.hub_v, (int32_t**)&h.hub_v)) ||
-        (rc = upload(&p, hp.hub_nchunks, (int32_t**)&h.hub_nchunks)) ||
-        (rc = upload(&p, hp.hub_tbase, (int64_t**)&h.hub_tbase)) ||
-        (rc = upload(&p, hp.hub_tmask, (uint32_t**)&h.hub_tmask)) ||
-        (rc = upload(&p, hp.hub_ubase, (int64_t**)&h.hub_ubase)) ||
-        (rc = zeroed(&p, (size_t)hp.table_slots, &h.gkeys)) || (rc = zeroed(&p, (size_t)hp.table_slots, &h.gvals)) ||
-        (rc = zeroed(&p, (size_t)hp.used_slots, &h.used)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.used_n)) ||
-        (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_best)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_done))) {
+        (rc = upload(&p, hp.hub_lbase, (int64_t**)&h.hub_lbase)) ||
+        (rc = upload(&p, hp.hub_nb, (int32_t**)&h.hub_nb)) ||
+        (rc = upload(&p, hp.item_hub, (int32_t**)&h.item_hub)) ||
+        (rc = upload(&p, hp.item_bucket, (int32_t**)&h.item_bucket)) ||
+        (rc = zeroed(&p, (size_t)hp.hub_labels, &h.hlab)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_best)) ||
+        (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_cand)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_state))) {
       free_plan(&p);
       return rc;
     }
+    h.nhubs = p.n_hubs;
+    h.nitems = (int32_t)hp.item_hub.size();
   }
   p.valid = true;
   return GLP_OK;
@@ -194,7 +217,8 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
 // --------------------------------------------------------------- launches
 template <class K>
 static int allow_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) GLP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  // static + dynamic shared memory above 48 KB needs the opt-in; set it always
+  GLP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   return GLP_OK;
 }
 
@@ -209,47 +233,71 @@ int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t*
     return GLP_OK;
   };
   int rc;
-  constexpr int kHubNT = 512, kBigNT = 512, kMidNT = 256;
+  if ((rc = mark(8, 0))) return rc;  // whole-step start
+  const unsigned kMaxGrid = 148 * 32;
+  constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 1024, kGroupU = 4;
+  if (S::kMajority && a.prev_changed) GLP_CUDA(cudaMemsetAsync(p.fail_counts, 0, 2 * sizeof(uint32_t), s));
   if (p.n_hubs) {
-    const size_t sm = 2ull * p.hub_cap * sizeof(uint32_t);
-    if ((rc = allow_smem(k_hub<kHubNT, W, S>, sm))) return rc;
+    const size_t sm = 2ull * kHubTable * sizeof(uint32_t);
+    if ((rc = allow_smem(k_hub_bucket<kBucketNT, W, S>, sm))) return rc;
     if ((rc = mark(5, 0))) return rc;
-    k_hub<kHubNT, W, S><<<p.n_chunks, kHubNT, sm, s>>>(a, p.hub, p.n_chunks, p.hub_cap, score);
+    const unsigned grid = (unsigned)std::min<int64_t>(p.n_chunks, kMaxGrid);
+    const unsigned hgrid = (unsigned)cdiv(p.n_hubs, 256);
+    if (S::kMajority && a.prev_changed) {
+      k_hub_majority<kHubNT, W><<<grid, kHubNT, 0, s>>>(a, p.hub, p.n_chunks);
+      ++*launches;
+    }
+    k_hub_decide<<<hgrid, 256, 0, s>>>(a, p.hub);
+    k_hub_gather<kHubNT><<<grid, kHubNT, 0, s>>>(a, p.hub, p.n_chunks);
+    k_hub_bucket<kBucketNT, W, S><<<(unsigned)std::min<int64_t>(p.hub.nitems, 148 * 4), kBucketNT, sm, s>>>(
+        a, p.hub, score);
+    k_hub_finalize<<<hgrid, 256, 0, s>>>(a, p.hub);
+    *launches += 4;
     if ((rc = mark(5, 1))) return rc;
+  }
+  if (S::kMajority && a.prev_changed && p.mb.n) {
+    if ((rc = mark(7, 0))) return rc;  // slot 7: the majority pre-pass
+    k_major_warp<W><<<(unsigned)std::min<int64_t>(cdiv((int64_t)p.mb.n * 32, 256), kMaxGrid), 256, 0, s>>>(
+        a, p.mb, p.tiers.mid_max, p.fmid, p.fbig);
+    if ((rc = mark(7, 1))) return rc;
     ++*launches;
   }
-  if (p.n_big) {
-    const size_t sm = 2ull * p.big_cap * sizeof(uint32_t);
+  if (p.big.n) {
+    const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
     if ((rc = allow_smem(k_big<kBigNT, W, S>, sm))) return rc;
     if ((rc = mark(4, 0))) return rc;
-    k_big<kBigNT, W, S><<<p.n_big, kBigNT, sm, s>>>(a, p.big, p.n_big, p.big_cap, score);
+    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, p.big, p.fbig, score);
     if ((rc = mark(4, 1))) return rc;
     ++*launches;
   }
-  if (p.n_mid) {
+  if (p.mid.n) {
     if ((rc = mark(3, 0))) return rc;
-    k_mid<512, kMidNT, W, S><<<(unsigned)cdiv(p.n_mid, kMidNT / 32), kMidNT, 0, s>>>(a, p.mid, p.n_mid, score);
+    k_mid<kMidCap, kMidNT, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.mid.n, kMidNT / 32), kMaxGrid), kMidNT, 0, s>>>(
+        a, p.mid, p.fmid, score);
     if ((rc = mark(3, 1))) return rc;
     ++*launches;
   }
-  if (p.n_g32) {
+  if (p.g32.n) {
     if ((rc = mark(2, 0))) return rc;
-    k_group<32, W, S><<<(unsigned)cdiv((int64_t)p.n_g32 * 32, 256), 256, 0, s>>>(a, p.g32, p.n_g32, score);
+    const int64_t warps = cdiv(p.g32.n, 1 * kGroupU);
+    k_group<32, kGroupU, W, S><<<(unsigned)cdiv(warps * 32, 256), 256, 0, s>>>(a, p.g32, score);
     if ((rc = mark(2, 1))) return rc;
     ++*launches;
   }
-  if (p.n_g16) {
+  if (p.g16.n) {
     if ((rc = mark(1, 0))) return rc;
-    k_group<16, W, S><<<(unsigned)cdiv((int64_t)p.n_g16 * 16, 256), 256, 0, s>>>(a, p.g16, p.n_g16, score);
+    const int64_t warps = cdiv(p.g16.n, 2 * kGroupU);
+    k_group<16, kGroupU, W, S><<<(unsigned)cdiv(warps * 32, 256), 256, 0, s>>>(a, p.g16, score);
     if ((rc = mark(1, 1))) return rc;
     ++*launches;
   }
-  if (p.n_tiny) {
+  if (p.tiny.n) {
     if ((rc = mark(0, 0))) return rc;
-    k_tiny<8, W, S><<<(unsigned)cdiv(p.n_tiny, 256), 256, 0, s>>>(a, p.tiny, p.n_tiny, score);
+    k_tiny<8, W, S><<<(unsigned)cdiv(p.tiny.n, 256), 256, 0, s>>>(a, p.tiny, score);
     if ((rc = mark(0, 1))) return rc;
     ++*launches;
   }
+  if ((rc = mark(8, 1))) return rc;  // whole-step stop
   GLP_CUDA(cudaGetLastError());
   return GLP_OK;
 }
@@ -269,6 +317,7 @@ struct RunCtx {
   std::vector<std::vector<bool>> ran;
   size_t used = 0;
   float tier_ms[8] = {};
+  std::vector<float> step_ms, step_tier;
   int64_t launches = 0;
   int iter_base = 0;
 
@@ -278,15 +327,16 @@ struct RunCtx {
         if (e) cudaEventDestroy(e);
   }
   // Events for the next step (nullptr when not timing).
+  static constexpr int kSlots = 9;  // tiers 0-5, aux 6, majority 7, whole step 8
   cudaEvent_t* step_events() {
     if (!timing) return nullptr;
     if (used == evs.size()) {
-      std::vector<cudaEvent_t> v(16, nullptr);
+      std::vector<cudaEvent_t> v(2 * kSlots, nullptr);
       for (auto& e : v)
         if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
       evs.push_back(v);
     }
-    ran.emplace_back(8, false);
+    ran.emplace_back(kSlots, false);
     return evs[used++].data();
   }
   void mark_ran(int tier) {
@@ -296,12 +346,14 @@ struct RunCtx {
     cudaEvent_t* ev = step_events();
     if (ev) {
       const DevicePlan& p = g->plan;
-      ran.back()[0] = p.n_tiny > 0;
-      ran.back()[1] = p.n_g16 > 0;
-      ran.back()[2] = p.n_g32 > 0;
-      ran.back()[3] = p.n_mid > 0;
-      ran.back()[4] = p.n_big > 0;
+      ran.back()[0] = p.tiny.n > 0;
+      ran.back()[1] = p.g16.n > 0;
+      ran.back()[2] = p.g32.n > 0;
+      ran.back()[3] = p.mid.n > 0;
+      ran.back()[4] = p.big.n > 0;
       ran.back()[5] = p.n_hubs > 0;
+      ran.back()[7] = p.mb.n > 0;
+      ran.back()[8] = true;
     }
     return StepLaunch{&g->plan, s, ev};
   }
@@ -309,12 +361,23 @@ struct RunCtx {
   int harvest() {
     if (!timing) return GLP_OK;
     GLP_CUDA(cudaStreamSynchronize(s));
+    step_ms.assign(used, 0.f);
+    step_tier.assign(used * 8, 0.f);
     for (size_t i = 0; i < used; ++i)
-      for (int t = 0; t < 8; ++t) {
+      for (int t = 0; t < kSlots; ++t) {
         if (!ran[i][t]) continue;
         float ms = 0;
-        GLP_CUDA(cudaEventElapsedTime(&ms, evs[i][2 * t], evs[i][2 * t + 1]));
-        tier_ms[t] += ms;
+        // a majority slot whose pre-pass was not launched this step has no events
+        if (cudaEventElapsedTime(&ms, evs[i][2 * t], evs[i][2 * t + 1]) != cudaSuccess) {
+          (void)cudaGetLastError();
+          continue;
+        }
+        if (t == 8) {
+          step_ms[i] = ms;
+        } else {
+          tier_ms[t] += ms;
+          step_tier[i * 8 + t] = ms;
+        }
       }
     return GLP_OK;
   }
@@ -397,7 +460,7 @@ static int run_classic(RunCtx& c, int32_t niter) {
   if (rc) return rc;
   for (int32_t it = 0; it < niter; ++it) {
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_lab[it & 1], g->d_lab[it & 1], g->d_lab[(it + 1) & 1],
-               g->d_changed + it, g->d_err};
+               g->d_changed + it, g->d_err, it > 0 ? g->d_changed + it - 1 : nullptr, g->n};
     if ((rc = launch_step<W>(c.launch(), a, ScoreClassic{}, &c.launches))) return rc;
     if ((rc = after_iter(c, it, g->d_lab[(it + 1) & 1]))) return rc;
   }
@@ -427,7 +490,7 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       }
       int32_t* lin = g->d_lab[it & 1];
       int32_t* lout = g->d_lab[(it + 1) & 1];
-      StepArgs a{g->d_off, g->d_cols, g->d_w, lin, lin, lout, g->d_changed + step, g->d_err};
+      StepArgs a{g->d_off, g->d_cols, g->d_w, lin, lin, lout, g->d_changed + step, g->d_err, nullptr, g->n};
       if ((rc = launch_step<W>(c.launch(), a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches))) return rc;
       if ((rc = c.aux_mark(0))) return rc;
       k_histogram<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(lout, g->n, vol_w);
@@ -463,7 +526,8 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
     ++c.launches;
     if ((rc = c.aux_mark(1))) return rc;
     GLP_CUDA(cudaGetLastError());
-    StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_spoken, lcur, lout, g->d_changed + it, g->d_err};
+    StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_spoken, lcur, lout, g->d_changed + it, g->d_err,
+               it > 0 ? g->d_changed + it - 1 : nullptr, g->n};
     if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) return rc;
     if ((rc = after_iter(c, it, lout))) return rc;
   }
@@ -497,13 +561,20 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
 }
 
 // ------------------------------------------------------------ validation
-__global__ void k_validate(const int32_t* __restrict__ cols, const int32_t* __restrict__ w, int64_t m, int32_t n,
-                           uint32_t* bad) {
+__global__ void k_validate(const int32_t* __restrict__ off, const int32_t* __restrict__ cols,
+                           const int32_t* __restrict__ w, int64_t m, int32_t n, uint32_t* bad) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
     const int32_t c = cols[j];
     if (c < 0 || c >= n) atomicOr(bad, 1u);
     if (w && w[j] < 0) atomicOr(bad, 2u);
   }
+  // the engine sums a vertex's weights in 32 bits
+  if (w)
+    for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+      int64_t sum = 0;
+      for (int32_t j = off[v]; j < off[v + 1]; ++j) sum += w[j];
+      if (sum >= 2147483648LL) atomicOr(bad, 4u);
+    }
 }
 
 int validate_csr_device(glp_graph* g) {
@@ -511,7 +582,7 @@ int validate_csr_device(glp_graph* g) {
   uint32_t* d_bad = nullptr;
   GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
   GLP_CUDA(cudaMemset(d_bad, 0, sizeof(uint32_t)));
-  k_validate<<<1184, 256>>>(g->d_cols, g->d_w, g->m, g->n, d_bad);
+  k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, d_bad);
   uint32_t bad = 0;
   cudaError_t e = cudaMemcpy(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost);
   cudaFree(d_bad);
@@ -522,6 +593,10 @@ int validate_csr_device(glp_graph* g) {
   }
   if (bad & 2u) {
     set_error("negative edge weight");
+    return GLP_EINVAL;
+  }
+  if (bad & 4u) {
+    set_error("a vertex's weight sum reaches 2^31");
     return GLP_EINVAL;
   }
   return GLP_OK;
@@ -659,10 +734,13 @@ int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t*
   GLP_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
   GLP_CUDA(cudaMalloc(&g->d_off, sizeof(int32_t) * ((size_t)n + 1)));
   GLP_CUDA(cudaMemcpy(g->d_off, g->h_off.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice));
-  GLP_CUDA(cudaMalloc(&g->d_cols, sizeof(int32_t) * std::max<int64_t>(m, 1)));
+  // 4 padding entries: tile kernels read columns as aligned 16-byte quads
+  GLP_CUDA(cudaMalloc(&g->d_cols, sizeof(int32_t) * (m + 4)));
+  GLP_CUDA(cudaMemset(g->d_cols + m, 0, sizeof(int32_t) * 4));
   if (m) GLP_CUDA(cudaMemcpy(g->d_cols, cols, sizeof(int32_t) * m, kind));
   if (weights) {
-    GLP_CUDA(cudaMalloc(&g->d_w, sizeof(int32_t) * std::max<int64_t>(m, 1)));
+    GLP_CUDA(cudaMalloc(&g->d_w, sizeof(int32_t) * (m + 4)));
+    GLP_CUDA(cudaMemset(g->d_w + m, 0, sizeof(int32_t) * 4));
     if (m) GLP_CUDA(cudaMemcpy(g->d_w, weights, sizeof(int32_t) * m, kind));
   }
   // validate columns (and weights) on the device
@@ -717,11 +795,6 @@ int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int
   if (rc) return rc;
   HostPlan hp;
   build_host_plan(offsets, n, t, &hp);
-  auto edges = [&](const std::vector<int32_t>& vs) {
-    int64_t e = 0;
-    for (int32_t v : vs) e += offsets[v + 1] - offsets[v];
-    return e;
-  };
   out[0] = hp.isolated;
   out[1] = (int64_t)hp.tiny.size();
   out[2] = (int64_t)hp.g16.size();
@@ -729,15 +802,9 @@ int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int
   out[4] = (int64_t)hp.mid.size();
   out[5] = (int64_t)hp.big.size();
   out[6] = (int64_t)hp.hub_v.size();
-  out[7] = (int64_t)hp.chunk_hub.size();
-  out[8] = 0;
-  out[9] = edges(hp.tiny);
-  out[10] = edges(hp.g16);
-  out[11] = edges(hp.g32);
-  out[12] = edges(hp.mid);
-  out[13] = edges(hp.big);
-  out[14] = edges(hp.hub_v);
-  out[15] = hp.table_slots;
+  out[7] = (int64_t)hp.item_hub.size();
+  for (int i = 0; i < 7; ++i) out[8 + i] = hp.edges[i];
+  out[15] = (int64_t)hp.chunk_hub.size();
   return GLP_OK;
 }
 
@@ -878,6 +945,11 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   if (out->tier_ms) {
     if ((rc = c.harvest())) return rc;
     for (int i = 0; i < 8; ++i) out->tier_ms[i] = c.tier_ms[i];
+    if (out->iter_ms)
+      for (size_t i = 0; i < c.step_ms.size() && (int32_t)i < total; ++i) out->iter_ms[i] = c.step_ms[i];
+    if (out->step_tier_ms)
+      for (size_t i = 0; i < c.step_ms.size() && (int32_t)i < total; ++i)
+        for (int t = 0; t < 8; ++t) out->step_tier_ms[i * 8 + t] = c.step_tier[i * 8 + t];
   }
   return check_err(g, c.s);
 }

@@ -20,11 +20,15 @@ int cuda_fail(cudaError_t e, const char* what);
   } while (0)
 
 // Degree-tier parameters after defaults and limits are applied.
+// Exact-count tier limits: a mid warp's table holds kMidCap slots, a big
+// block's table kBigCap slots (both at most half full).
+constexpr int kMidCap = 512, kBigCap = 8192;
+
 struct TierParams {
-  int32_t tiny_max = 8;    // <= 8 (register tier width)
-  int32_t mid_max = 256;   // <= 256 (per-warp table of 512 slots)
-  int32_t big_max = 4096;  // <= 8192
-  int32_t hub_chunk = 4096;
+  int32_t tiny_max = 8;       // <= 8
+  int32_t mid_max = 256;      // <= kMidCap / 2
+  int32_t big_max = 4096;     // <= kBigCap / 2
+  int32_t hub_chunk = 16384;  // edges per hub streaming block
   bool operator==(const TierParams& o) const {
     return tiny_max == o.tiny_max && mid_max == o.mid_max && big_max == o.big_max && hub_chunk == o.hub_chunk;
   }
@@ -33,26 +37,28 @@ int resolve_tiers(const glp_params* p, TierParams* t);
 
 // Host-side plan (pure function of the offsets and the tier parameters).
 struct HostPlan {
-  std::vector<int32_t> tiny, g16, g32, mid, big;  // vertex lists (ascending ids)
+  std::vector<int32_t> tiny, g16, g32, mid, big, mb;  // vertex lists (ascending ids); mb = mid + big
   int64_t isolated = 0;
+  int64_t edges[7] = {0, 0, 0, 0, 0, 0, 0};  // per tier, as the vertex counts of glp_graph_plan
   // hubs
-  std::vector<int32_t> hub_v, hub_nchunks;
-  std::vector<int64_t> hub_tbase, hub_ubase;
-  std::vector<uint32_t> hub_tmask;
+  std::vector<int32_t> hub_v, hub_nb;
+  std::vector<int64_t> hub_lbase;
   std::vector<int32_t> chunk_hub, chunk_begin, chunk_end;
-  int64_t table_slots = 0, used_slots = 0;
+  std::vector<int32_t> item_hub, item_bucket;
+  int64_t hub_labels = 0;
 };
 void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPlan* hp);
 
 struct DevicePlan {
   TierParams tiers;
   bool valid = false;
-  int32_t n_tiny = 0, n_g16 = 0, n_g32 = 0, n_mid = 0, n_big = 0, n_hubs = 0, n_chunks = 0;
+  Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{};
+  FailList fmid{}, fbig{};
+  uint32_t* fail_counts = nullptr;  // [2] fmid, fbig counts
+  int32_t n_hubs = 0, n_chunks = 0;
   int64_t isolated = 0;
-  int32_t *tiny = nullptr, *g16 = nullptr, *g32 = nullptr, *mid = nullptr, *big = nullptr;
   HubPlan hub{};
   std::vector<void*> allocs;
-  uint32_t big_cap = 0, hub_cap = 0;
 };
 
 // Launch configuration of one synchronous step.

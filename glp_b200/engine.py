@@ -26,7 +26,7 @@ import torch
 from . import _lib
 from .graphs import CSR, from_numpy
 
-TIERS = ("tiny", "group16", "group32", "mid", "big", "hub", "aux", "-")
+TIERS = ("tiny", "group16", "group32", "mid", "big", "hub", "aux", "majority")
 
 
 def make_params(**kw) -> _lib.Params:
@@ -61,6 +61,8 @@ class Result:
     slpa_ncomm: np.ndarray | None = None
     slpa_mem: np.ndarray | None = None
     vol: np.ndarray | None = None
+    iter_ms: np.ndarray | None = None
+    step_tier_ms: np.ndarray | None = None
     extra: dict = field(default_factory=dict)
 
 
@@ -149,8 +151,8 @@ class Graph:
         names = ("isolated", "tiny", "group16", "group32", "mid", "big", "hub")
         d = {f"v_{k}": out[i] for i, k in enumerate(names)}
         d.update({f"e_{k}": out[8 + i] for i, k in enumerate(names)})
-        d["hub_blocks"] = out[7]
-        d["hub_table_slots"] = out[15]
+        d["hub_buckets"] = out[7]
+        d["hub_chunks"] = out[15]
         return d
 
     def check(self) -> None:
@@ -174,8 +176,12 @@ class Graph:
         if not p.async_:
             out.changed = changed.ctypes.data
         tier_ms = np.zeros(8, dtype=np.float32)
+        iter_ms = np.zeros(max(total, 1), dtype=np.float32)
+        step_tier = np.zeros((max(total, 1), 8), dtype=np.float32)
         if profile:
             out.tier_ms = tier_ms.ctypes.data
+            out.iter_ms = iter_ms.ctypes.data
+            out.step_tier_ms = step_tier.ctypes.data
         launches = np.zeros(1, dtype=np.int64)
         out.launches = launches.ctypes.data
         res_extra = {}
@@ -210,6 +216,9 @@ class Graph:
         if cb_err:
             raise cb_err[0]
         _lib.check(rc)
+        if profile:
+            res_extra["iter_ms"] = iter_ms[:total]
+            res_extra["step_tier_ms"] = step_tier[:total]
         return Result(labels=labels, changed=changed[:total], seconds=dt,
                       tier_ms=tier_ms if profile else None, launches=int(launches[0]), vol=vol, **res_extra)
 

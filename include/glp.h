@@ -78,10 +78,10 @@ typedef struct glp_params {
   /* method 4 */
   int32_t hooks;                  /* GLP_HOOKS_* */
   /* degree tiers (0 = engine default / autotuned) */
-  int32_t tiny_max;               /* thread per vertex up to this degree */
-  int32_t mid_max;                /* warp per vertex up to this degree */
-  int32_t big_max;                /* block per vertex up to this degree; above: hub chunks */
-  int32_t hub_chunk;              /* edges per hub block */
+  int32_t tiny_max;               /* thread per vertex up to this degree (<= 8) */
+  int32_t mid_max;                /* warp per vertex up to this degree (32..256) */
+  int32_t big_max;                /* block per vertex up to this degree (mid_max..4096); above: hubs */
+  int32_t hub_chunk;              /* edges per hub streaming block (256..65536) */
   int32_t use_graph;              /* capture the iteration loop in a CUDA graph */
   int32_t async;                  /* 1: enqueue on the stream and return without
                                      synchronising (device outputs only, no
@@ -103,10 +103,13 @@ typedef struct glp_outputs {
   int32_t* slpa_mem;    /* [slpa_T][n] speaker memory, -1 = empty */
   int32_t* vol;         /* [n] layered: label volumes after the last iteration */
   int64_t* changed;     /* [iterations] labels changed per iteration (host) */
-  float* tier_ms;       /* [8] host: summed device ms per kernel tier (tiny, group16,
-                           group32, mid, big, hub, aux, -), timed with CUDA events
-                           on the run's stream; NULL = no per-tier events */
+  float* tier_ms;       /* [8] host: summed device ms per kernel group (tiny, group16,
+                           group32, mid, big, hub, aux, majority pre-pass), timed
+                           with CUDA events on the run's stream; NULL = none */
   int64_t* launches;    /* [1] host: kernels this run launched */
+  float* iter_ms;       /* [iterations] host: device ms of each iteration's step
+                           kernels (timed like tier_ms; needs tier_ms) */
+  float* step_tier_ms;  /* [iterations][8] host: per-iteration tier_ms (needs tier_ms) */
   int32_t on_device;    /* 1: labels/slpa/vol pointers are device pointers */
 } glp_outputs;
 
@@ -126,9 +129,9 @@ int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t*
 void glp_graph_destroy(glp_graph* g);
 int glp_graph_info(const glp_graph* g, int32_t* n, int64_t* m, int32_t* max_degree);
 /* Degree-tier plan for these params.  out[0..6]: vertices per tier
- * [isolated, tiny, group16, group32, mid, big, hub]; out[7]: hub blocks;
- * out[8..14]: CSR entries (edges) per tier in the same order; out[15]:
- * global hub-table slots.  Mirrors the bin report of
+ * [isolated, tiny, group16, group32, mid, big, hub]; out[7]: hub hash
+ * buckets; out[8..14]: CSR entries (edges) per tier in the same order;
+ * out[15]: hub streaming chunks.  Mirrors the bin report of
  * prop/classicLprop.cuh:213-227. */
 int glp_graph_plan(glp_graph* g, const glp_params* p, int64_t out[16]);
 /* The same plan computed from host offsets alone (no device needed). */

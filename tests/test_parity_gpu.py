@@ -29,6 +29,8 @@ def _cases():
         "cycle": cycle(31),
         "star": star(100),
         "star_ring_3000": _star_ring(3000),
+        "star_ring_10000": _star_ring(10000),
+        "star_ring_20000": _star_ring(20000),
         "two_cliques": two_cliques(20),
         "ladder": degree_ladder(BOUNDARY_DEGREES),
         "isolated_only": (np.zeros(6, np.int32), np.zeros(0, np.int32)),
@@ -46,7 +48,7 @@ CASES = _cases()
 TIERS = {
     "default": {},
     "small_hubs": dict(tiny_max=4, mid_max=64, big_max=128, hub_chunk=256),
-    "no_tiny": dict(tiny_max=-1, mid_max=32, big_max=32, hub_chunk=512),
+    "mostly_hubs": dict(tiny_max=-1, mid_max=32, big_max=32, hub_chunk=512),
 }
 
 
@@ -74,8 +76,8 @@ def test_classic_per_iteration(case, tier):
         prev = otr[it]
 
 
-@pytest.mark.parametrize("tier", ["default", "small_hubs"])
-@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "planted20k"])
+@pytest.mark.parametrize("tier", ["default", "small_hubs", "mostly_hubs"])
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "star_ring_10000", "planted20k"])
 def test_weighted_per_iteration(case, tier):
     off, cols = CASES[case]
     w = (np.arange(len(cols), dtype=np.int64) * 2654435761 % 16 + 1).astype(np.int32)
@@ -89,8 +91,9 @@ def test_weighted_per_iteration(case, tier):
         np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
 
 
-@pytest.mark.parametrize("tier", ["default", "small_hubs"])
-@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "two_cliques", "planted20k"])
+@pytest.mark.parametrize("tier", ["default", "small_hubs", "mostly_hubs"])
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "star_ring_10000", "two_cliques",
+                                  "planted20k"])
 def test_layered_per_iteration(case, tier):
     off, cols = CASES[case]
     dstar = [2, 3, 5, 9, 17]
