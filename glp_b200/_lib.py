@@ -25,6 +25,7 @@ GLP_EAGAIN = -9
 METHOD_CLASSIC, METHOD_LAYERED, METHOD_SLPA, METHOD_USER = 1, 2, 3, 4
 BACKEND_EXACT, BACKEND_CM, BACKEND_FA = 0, 1, 2
 HOOKS_CLASSIC, HOOKS_LAYERED, HOOKS_WEIGHTED_DEGREE = 0, 1, 2
+GRAPH_SYMMETRIC = 1
 MAX_LAYERS = 32
 
 _ERRNAMES = {
@@ -87,6 +88,8 @@ SIGNATURES = {
     "glp_params_default": (C.c_int, [C.POINTER(Params)]),
     "glp_graph_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32,
                                    C.POINTER(C.c_void_p)]),
+    "glp_graph_create_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32,
+                                      C.c_uint32, C.POINTER(C.c_void_p)]),
     "glp_graph_destroy": (None, [C.c_void_p]),
     "glp_graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "glp_graph_plan": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(C.c_int64)]),

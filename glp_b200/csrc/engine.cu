@@ -184,13 +184,30 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
       (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
       (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
-      (rc = zeroed(&p, 2, &p.fail_counts)) || (rc = zeroed(&p, std::max<size_t>(hp.mid.size(), 1), &p.fmid.ids)) ||
-      (rc = zeroed(&p, std::max<size_t>(hp.big.size(), 1), &p.fbig.ids))) {
+      (rc = zeroed(&p, 9, &p.counts)) || (rc = zeroed(&p, std::max<size_t>(hp.mid.size(), 1), &p.fmid.ids)) ||
+      (rc = zeroed(&p, std::max<size_t>(hp.big.size(), 1), &p.fbig.ids)) || (rc = zeroed(&p, 1, &p.d_mode)) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.front.act)) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[0])) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[1]))) {
     free_plan(&p);
     return rc;
   }
-  p.fmid.count = p.fail_counts;
-  p.fbig.count = p.fail_counts + 1;
+  g->epoch = 0;  // fresh marks
+  p.fmid.count = p.counts;
+  p.fbig.count = p.counts + 1;
+  p.front.tiny_max = t.tiny_max;
+  p.front.mid_max = t.mid_max;
+  p.front.big_max = t.big_max;
+  {
+    const std::vector<int32_t>* lists[5] = {&hp.tiny, &hp.g16, &hp.g32, &hp.mid, &hp.big};
+    for (int k = 0; k < 5; ++k) {
+      if ((rc = zeroed(&p, std::max<size_t>(lists[k]->size(), 1), &p.front.tier[k].ids))) {
+        free_plan(&p);
+        return rc;
+      }
+      p.front.tier[k].count = p.counts + 2 + k;
+    }
+  }
   p.n_hubs = (int32_t)hp.hub_v.size();
   p.n_chunks = (int32_t)hp.chunk_hub.size();
   if (p.n_hubs) {
@@ -228,76 +245,108 @@ template <bool W, class S>
 int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t* launches) {
   const DevicePlan& p = *L.plan;
   cudaStream_t s = L.stream;
-  auto mark = [&](int i, int which) -> int {
-    if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[2 * i + which], s));
+  auto mark_on = [&](cudaStream_t st, int i, int which) -> int {
+    if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[2 * i + which], st));
     return GLP_OK;
   };
   int rc;
-  if ((rc = mark(8, 0))) return rc;  // whole-step start
   const unsigned kMaxGrid = 148 * 32;
+  if ((rc = mark_on(s, 8, 0))) return rc;  // whole-step start
+  const bool modal = a.mode != nullptr;
+  if (modal) {
+    GLP_CUDA(cudaMemsetAsync(p.counts, 0, 7 * sizeof(uint32_t), s));
+    k_step_mode<<<1, 1, 0, s>>>(L.prev_changed, a.n, L.allow_majority, L.allow_frontier, p.d_mode);
+    ++*launches;
+    if (L.allow_frontier && L.front.chg_in) {
+      const unsigned fgrid = 148 * 16;
+      k_frontier_push<<<fgrid, 256, 0, s>>>(a, L.front);
+      k_frontier_copy<<<fgrid, 256, 0, s>>>(a, L.front);
+      *launches += 2;
+      if (p.n_hubs) {
+        k_frontier_hubs<<<(unsigned)cdiv(p.n_hubs, 256), 256, 0, s>>>(a, L.front, p.hub);
+        ++*launches;
+      }
+    }
+  }
+  auto work = [&](const Verts& all, int k, const FailList* major) {
+    TierWork tw{all, major ? *major : FailList{nullptr, nullptr}, p.front.tier[k]};
+    return tw;
+  };
+  // fork: hubs on aux[0], the small tiers on aux[1], the rest here
+  GLP_CUDA(cudaEventRecord(L.fork, s));
+  GLP_CUDA(cudaStreamWaitEvent(L.aux[0], L.fork, 0));
+  GLP_CUDA(cudaStreamWaitEvent(L.aux[1], L.fork, 0));
   constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 1024, kGroupU = 4;
-  if (S::kMajority && a.prev_changed) GLP_CUDA(cudaMemsetAsync(p.fail_counts, 0, 2 * sizeof(uint32_t), s));
   if (p.n_hubs) {
     const size_t sm = 2ull * kHubTable * sizeof(uint32_t);
     if ((rc = allow_smem(k_hub_bucket<kBucketNT, W, S>, sm))) return rc;
-    if ((rc = mark(5, 0))) return rc;
+    if ((rc = mark_on(L.aux[0], 5, 0))) return rc;
     const unsigned grid = (unsigned)std::min<int64_t>(p.n_chunks, kMaxGrid);
     const unsigned hgrid = (unsigned)cdiv(p.n_hubs, 256);
-    if (S::kMajority && a.prev_changed) {
-      k_hub_majority<kHubNT, W><<<grid, kHubNT, 0, s>>>(a, p.hub, p.n_chunks);
+    if (L.allow_majority && modal) {
+      k_hub_majority<kHubNT, W><<<grid, kHubNT, 0, L.aux[0]>>>(a, p.hub, p.n_chunks);
       ++*launches;
     }
-    k_hub_decide<<<hgrid, 256, 0, s>>>(a, p.hub);
-    k_hub_gather<kHubNT><<<grid, kHubNT, 0, s>>>(a, p.hub, p.n_chunks);
-    k_hub_bucket<kBucketNT, W, S><<<(unsigned)std::min<int64_t>(p.hub.nitems, 148 * 4), kBucketNT, sm, s>>>(
+    k_hub_decide<<<hgrid, 256, 0, L.aux[0]>>>(a, p.hub);
+    k_hub_gather<kHubNT><<<grid, kHubNT, 0, L.aux[0]>>>(a, p.hub, p.n_chunks);
+    k_hub_bucket<kBucketNT, W, S><<<(unsigned)std::min<int64_t>(p.hub.nitems, 148 * 4), kBucketNT, sm, L.aux[0]>>>(
         a, p.hub, score);
-    k_hub_finalize<<<hgrid, 256, 0, s>>>(a, p.hub);
+    k_hub_finalize<<<hgrid, 256, 0, L.aux[0]>>>(a, p.hub);
     *launches += 4;
-    if ((rc = mark(5, 1))) return rc;
+    if ((rc = mark_on(L.aux[0], 5, 1))) return rc;
   }
-  if (S::kMajority && a.prev_changed && p.mb.n) {
-    if ((rc = mark(7, 0))) return rc;  // slot 7: the majority pre-pass
+  if (L.allow_majority && modal && p.mb.n) {
+    if ((rc = mark_on(s, 7, 0))) return rc;  // slot 7: the majority pre-pass
     k_major_warp<W><<<(unsigned)std::min<int64_t>(cdiv((int64_t)p.mb.n * 32, 256), kMaxGrid), 256, 0, s>>>(
         a, p.mb, p.tiers.mid_max, p.fmid, p.fbig);
-    if ((rc = mark(7, 1))) return rc;
+    if ((rc = mark_on(s, 7, 1))) return rc;
     ++*launches;
   }
   if (p.big.n) {
     const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
     if ((rc = allow_smem(k_big<kBigNT, W, S>, sm))) return rc;
-    if ((rc = mark(4, 0))) return rc;
-    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, p.big, p.fbig, score);
-    if ((rc = mark(4, 1))) return rc;
+    if ((rc = mark_on(s, 4, 0))) return rc;
+    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, work(p.big, 4, &p.fbig),
+                                                                                          score);
+    if ((rc = mark_on(s, 4, 1))) return rc;
     ++*launches;
   }
   if (p.mid.n) {
-    if ((rc = mark(3, 0))) return rc;
+    if ((rc = mark_on(s, 3, 0))) return rc;
     k_mid<kMidCap, kMidNT, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.mid.n, kMidNT / 32), kMaxGrid), kMidNT, 0, s>>>(
-        a, p.mid, p.fmid, score);
-    if ((rc = mark(3, 1))) return rc;
+        a, work(p.mid, 3, &p.fmid), score);
+    if ((rc = mark_on(s, 3, 1))) return rc;
     ++*launches;
   }
   if (p.g32.n) {
-    if ((rc = mark(2, 0))) return rc;
+    if ((rc = mark_on(L.aux[1], 2, 0))) return rc;
     const int64_t warps = cdiv(p.g32.n, 1 * kGroupU);
-    k_group<32, kGroupU, W, S><<<(unsigned)cdiv(warps * 32, 256), 256, 0, s>>>(a, p.g32, score);
-    if ((rc = mark(2, 1))) return rc;
+    k_group<32, kGroupU, W, S><<<(unsigned)std::min<int64_t>(cdiv(warps * 32, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
+        a, work(p.g32, 2, nullptr), score);
+    if ((rc = mark_on(L.aux[1], 2, 1))) return rc;
     ++*launches;
   }
   if (p.g16.n) {
-    if ((rc = mark(1, 0))) return rc;
+    if ((rc = mark_on(L.aux[1], 1, 0))) return rc;
     const int64_t warps = cdiv(p.g16.n, 2 * kGroupU);
-    k_group<16, kGroupU, W, S><<<(unsigned)cdiv(warps * 32, 256), 256, 0, s>>>(a, p.g16, score);
-    if ((rc = mark(1, 1))) return rc;
+    k_group<16, kGroupU, W, S><<<(unsigned)std::min<int64_t>(cdiv(warps * 32, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
+        a, work(p.g16, 1, nullptr), score);
+    if ((rc = mark_on(L.aux[1], 1, 1))) return rc;
     ++*launches;
   }
   if (p.tiny.n) {
-    if ((rc = mark(0, 0))) return rc;
-    k_tiny<8, W, S><<<(unsigned)cdiv(p.tiny.n, 256), 256, 0, s>>>(a, p.tiny, score);
-    if ((rc = mark(0, 1))) return rc;
+    if ((rc = mark_on(L.aux[1], 0, 0))) return rc;
+    k_tiny<8, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.tiny.n, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
+        a, work(p.tiny, 0, nullptr), score);
+    if ((rc = mark_on(L.aux[1], 0, 1))) return rc;
     ++*launches;
   }
-  if ((rc = mark(8, 1))) return rc;  // whole-step stop
+  // join
+  GLP_CUDA(cudaEventRecord(L.join[0], L.aux[0]));
+  GLP_CUDA(cudaEventRecord(L.join[1], L.aux[1]));
+  GLP_CUDA(cudaStreamWaitEvent(s, L.join[0], 0));
+  GLP_CUDA(cudaStreamWaitEvent(s, L.join[1], 0));
+  if ((rc = mark_on(s, 8, 1))) return rc;  // whole-step stop
   GLP_CUDA(cudaGetLastError());
   return GLP_OK;
 }
@@ -355,7 +404,7 @@ struct RunCtx {
       ran.back()[7] = p.mb.n > 0;
       ran.back()[8] = true;
     }
-    return StepLaunch{&g->plan, s, ev};
+    return StepLaunch{&g->plan, s, ev, {g->aux[0], g->aux[1]}, g->fork, {g->join[0], g->join[1]}};
   }
   cudaEvent_t* current() { return timing && used ? evs[used - 1].data() : nullptr; }
   int harvest() {
@@ -453,15 +502,49 @@ static int init_labels(RunCtx& c) {
   return GLP_OK;
 }
 
+// Decides (once per handle) whether the CSR stores every edge both ways.
+static int ensure_symmetric(glp_graph* g) {
+  if (g->symmetric >= 0) return GLP_OK;
+  g->symmetric = 0;
+  if (g->m == 0) {
+    g->symmetric = 1;
+    return GLP_OK;
+  }
+  uint32_t* d_bad = nullptr;
+  GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
+  GLP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), g->stream));
+  k_check_symmetric<<<148 * 16, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, g->m, d_bad);
+  uint32_t bad = 1;
+  GLP_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, g->stream));
+  GLP_CUDA(cudaStreamSynchronize(g->stream));
+  cudaFree(d_bad);
+  g->symmetric = bad == 0 ? 1 : 0;
+  return GLP_OK;
+}
+
 template <bool W>
 static int run_classic(RunCtx& c, int32_t niter) {
   glp_graph* g = c.g;
   int rc = init_labels(c);
   if (rc) return rc;
   for (int32_t it = 0; it < niter; ++it) {
+    const bool fr = g->symmetric == 1;
+    DevicePlan& p = g->plan;
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_lab[it & 1], g->d_lab[it & 1], g->d_lab[(it + 1) & 1],
-               g->d_changed + it, g->d_err, it > 0 ? g->d_changed + it - 1 : nullptr, g->n};
-    if ((rc = launch_step<W>(c.launch(), a, ScoreClassic{}, &c.launches))) return rc;
+               g->d_changed + it, g->d_err, p.d_mode, g->n, fr ? p.chg[it & 1] : nullptr,
+               fr ? p.counts + 7 + (it & 1) : nullptr};
+    if (fr) GLP_CUDA(cudaMemsetAsync(p.counts + 7 + (it & 1), 0, sizeof(uint32_t), c.s));
+    StepLaunch L = c.launch();
+    L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
+    L.allow_majority = 1;
+    L.allow_frontier = fr;
+    if (fr && it > 0) {
+      L.front = p.front;
+      L.front.epoch = ++g->epoch;
+      L.front.chg_in = p.chg[(it - 1) & 1];
+      L.front.chg_in_n = p.counts + 7 + ((it - 1) & 1);
+    }
+    if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) return rc;
     if ((rc = after_iter(c, it, g->d_lab[(it + 1) & 1]))) return rc;
   }
   return GLP_OK;
@@ -490,7 +573,8 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       }
       int32_t* lin = g->d_lab[it & 1];
       int32_t* lout = g->d_lab[(it + 1) & 1];
-      StepArgs a{g->d_off, g->d_cols, g->d_w, lin, lin, lout, g->d_changed + step, g->d_err, nullptr, g->n};
+      StepArgs a{g->d_off, g->d_cols, g->d_w, lin,     lin,   lout, g->d_changed + step, g->d_err,
+                 nullptr, g->n,   nullptr, nullptr};  // full counting every step
       if ((rc = launch_step<W>(c.launch(), a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches))) return rc;
       if ((rc = c.aux_mark(0))) return rc;
       k_histogram<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(lout, g->n, vol_w);
@@ -527,7 +611,9 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
     if ((rc = c.aux_mark(1))) return rc;
     GLP_CUDA(cudaGetLastError());
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_spoken, lcur, lout, g->d_changed + it, g->d_err,
-               it > 0 ? g->d_changed + it - 1 : nullptr, g->n};
+               g->plan.d_mode, g->n, nullptr, nullptr};
+    L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
+    L.allow_majority = 1;  // the listener mode; spoken labels change every step: no frontier
     if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) return rc;
     if ((rc = after_iter(c, it, lout))) return rc;
   }
@@ -695,6 +781,11 @@ int glp_params_default(glp_params* p) {
 
 int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n, int64_t m,
                      int32_t on_device, glp_graph** out) {
+  return glp_graph_create_ex(offsets, cols, weights, n, m, on_device, 0u, out);
+}
+
+int glp_graph_create_ex(const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n, int64_t m,
+                        int32_t on_device, uint32_t flags, glp_graph** out) {
   if (!out) {
     set_error("out is NULL");
     return GLP_EINVAL;
@@ -732,6 +823,11 @@ int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t*
   }
   g->max_degree = maxd;
   GLP_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  GLP_CUDA(cudaStreamCreateWithFlags(&g->aux[0], cudaStreamNonBlocking));
+  GLP_CUDA(cudaStreamCreateWithFlags(&g->aux[1], cudaStreamNonBlocking));
+  GLP_CUDA(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
+  GLP_CUDA(cudaEventCreateWithFlags(&g->join[0], cudaEventDisableTiming));
+  GLP_CUDA(cudaEventCreateWithFlags(&g->join[1], cudaEventDisableTiming));
   GLP_CUDA(cudaMalloc(&g->d_off, sizeof(int32_t) * ((size_t)n + 1)));
   GLP_CUDA(cudaMemcpy(g->d_off, g->h_off.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice));
   // 4 padding entries: tile kernels read columns as aligned 16-byte quads
@@ -745,6 +841,7 @@ int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t*
   }
   // validate columns (and weights) on the device
   if ((rc = validate_csr_device(g.get()))) return rc;
+  if (flags & GLP_GRAPH_SYMMETRIC) g->symmetric = 1;
   *out = g.release();
   return GLP_OK;
 }
@@ -766,6 +863,11 @@ void glp_graph_destroy(glp_graph* g) {
   cudaFree(g->d_hook_keys);
   cudaFree(g->d_hook_vals);
   if (g->stream) cudaStreamDestroy(g->stream);
+  for (cudaStream_t st : g->aux)
+    if (st) cudaStreamDestroy(st);
+  if (g->fork) cudaEventDestroy(g->fork);
+  for (cudaEvent_t e : g->join)
+    if (e) cudaEventDestroy(e);
   delete g;
 }
 
@@ -909,6 +1011,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;
+  if (method == GLP_METHOD_CLASSIC && (rc = ensure_symmetric(g))) return rc;
   switch (method) {
     case GLP_METHOD_CLASSIC:
       rc = W ? run_classic<true>(c, niter) : run_classic<false>(c, niter);

@@ -54,7 +54,13 @@ struct DevicePlan {
   bool valid = false;
   Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{};
   FailList fmid{}, fbig{};
-  uint32_t* fail_counts = nullptr;  // [2] fmid, fbig counts
+  // list counters: [majority mid, majority big, frontier tiny, g16, g32, mid,
+  // big] are zeroed at the start of every step; [7 + s] counts the changed
+  // list chg[s] that steps of parity s append to
+  uint32_t* counts = nullptr;
+  int32_t* chg[2] = {nullptr, nullptr};
+  Frontier front{};
+  int32_t* d_mode = nullptr;
   int32_t n_hubs = 0, n_chunks = 0;
   int64_t isolated = 0;
   HubPlan hub{};
@@ -62,10 +68,19 @@ struct DevicePlan {
 };
 
 // Launch configuration of one synchronous step.
+// The step forks onto two auxiliary streams (hubs; small tiers) and joins
+// back before it returns: the tier kernels write disjoint vertices.
 struct StepLaunch {
   const DevicePlan* plan;
   cudaStream_t stream;
-  cudaEvent_t* ev;  // nullable: 7 pairs of (start, stop) for per-tier timing
+  cudaEvent_t* ev;  // nullable: (start, stop) pairs for per-tier timing
+  cudaStream_t aux[2];
+  cudaEvent_t fork, join[2];
+  // step-mode inputs (k_step_mode): previous step's changed count (nullptr
+  // in the first step) and which shortcuts the method admits
+  const unsigned long long* prev_changed = nullptr;
+  int allow_majority = 0, allow_frontier = 0;
+  Frontier front{};  // this step's frontier inputs (front.chg_in set from the second step)
 };
 
 template <bool W, class S>
@@ -96,4 +111,9 @@ struct glp_graph {
   // method-4 spill tables (2 slots per CSR entry), allocated on first use
   uint32_t* d_hook_keys = nullptr;
   double* d_hook_vals = nullptr;
+  int symmetric = -1;  // -1 unknown, 0 no, 1 yes (every edge stored both ways)
+  uint32_t epoch = 0;  // frontier mark of the last step
+  // auxiliary streams and fork/join events of a step
+  cudaStream_t aux[2] = {nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
 };

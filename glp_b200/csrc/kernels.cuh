@@ -40,14 +40,58 @@ struct StepArgs {
   int32_t* lout;
   unsigned long long* changed;
   uint32_t* err;
-  // majority pre-pass switch: on when prev_changed is set and the previous
-  // step changed fewer than n/20 labels
-  const unsigned long long* prev_changed;
+  // this step's mode, set on the device by k_step_mode (nullptr: full)
+  const int32_t* mode;
   int32_t n;
+  // vertices whose label changed this step are appended here (nullable)
+  int32_t* chg_out;
+  uint32_t* chg_out_n;
 };
 
-__device__ __forceinline__ bool use_majority(const StepArgs& a) {
-  return a.prev_changed != nullptr && (*a.prev_changed) * 20ull < (unsigned long long)a.n;
+// Counts (and, when a.chg_out is set, lists) the vertices whose label changed.
+// Every lane of the warp calls it; v is only read when changed.
+__device__ __forceinline__ void record_changes(const StepArgs& a, bool changed, int32_t v) {
+  const uint32_t m = __ballot_sync(kFull, changed);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) {
+    atomicAdd(a.changed, (unsigned long long)__popc(m));
+    if (a.chg_out) base = atomicAdd(a.chg_out_n, (uint32_t)__popc(m));
+  }
+  if (a.chg_out) {
+    base = __shfl_sync(kFull, base, leader);
+    if (changed) a.chg_out[base + __popc(m & ((1u << lane) - 1u))] = v;
+  }
+}
+
+// The same for one thread deciding alone.
+__device__ __forceinline__ void record_change(const StepArgs& a, int32_t v) {
+  atomicAdd(a.changed, 1ull);
+  if (a.chg_out) a.chg_out[atomicAdd(a.chg_out_n, 1u)] = v;
+}
+
+// Step modes.  Full: every vertex counts exactly.  Majority: a streaming
+// pre-pass decides vertices whose own label holds a strict majority and
+// lists the others.  Frontier: only vertices with a neighbour that changed in
+// the previous step are recomputed; the others provably keep their label.
+enum : int32_t { kModeFull = 0, kModeMajority = 1, kModeFrontier = 2 };
+
+__device__ __forceinline__ int32_t step_mode(const StepArgs& a) { return a.mode ? *a.mode : kModeFull; }
+__device__ __forceinline__ bool use_majority(const StepArgs& a) { return step_mode(a) == kModeMajority; }
+
+// Picks the mode from the previous step's changed count: frontier below n/20
+// changes (when allowed), majority below n/4 (when allowed), else full.
+__global__ void k_step_mode(const unsigned long long* prev_changed, int32_t n, int allow_majority,
+                            int allow_frontier, int32_t* mode) {
+  int32_t m = kModeFull;
+  if (prev_changed) {
+    const unsigned long long c = *prev_changed;
+    if (allow_frontier && c * 20ull < (unsigned long long)n) m = kModeFrontier;
+    else if (allow_majority && c * 4ull < (unsigned long long)n) m = kModeMajority;
+  }
+  *mode = m;
 }
 
 // The vertices of one tier: explicit ids, or the contiguous range
@@ -59,18 +103,30 @@ struct Verts {
   __device__ __forceinline__ int32_t operator[](int64_t i) const { return ids ? ids[i] : base + (int32_t)i; }
 };
 
-// Vertices the majority pre-pass could not decide.
+// A device-built vertex list (majority failures, frontier members).
 struct FailList {
   int32_t* ids;
   uint32_t* count;
 };
 
-// The work of an exact-count kernel: its tier, or the tier's fail list when
-// the pre-pass ran.
-__device__ __forceinline__ int32_t work_size(const StepArgs& a, const Verts& vs, const FailList& fl, bool* listed) {
-  *listed = use_majority(a);
-  return *listed ? (int32_t)*fl.count : vs.n;
-}
+// The vertices an exact-count kernel works on this step: the whole tier
+// (full mode), the tier's majority failures (majority mode, mid/big only) or
+// the tier's frontier members (frontier mode).
+struct TierWork {
+  Verts all;
+  FailList major;  // ids == nullptr: the tier has no pre-pass
+  FailList front;
+  __device__ __forceinline__ int32_t size(int32_t mode) const {
+    if (mode == kModeFrontier && front.ids) return (int32_t)*front.count;
+    if (mode == kModeMajority && major.ids) return (int32_t)*major.count;
+    return all.n;
+  }
+  __device__ __forceinline__ int32_t at(int32_t mode, int64_t i) const {
+    if (mode == kModeFrontier && front.ids) return front.ids[i];
+    if (mode == kModeMajority && major.ids) return major.ids[i];
+    return all[i];
+  }
+};
 
 // score(l, k) for classic LP: the count itself.  A label holding more than
 // half of the neighbourhood weight is then the unique maximum, so the
@@ -111,11 +167,16 @@ __device__ __forceinline__ unsigned long long pack_best(const Best& b, uint32_t*
 
 // ---------------------------------------------------------------- tiny tier
 template <int TMAX, bool W, class S>
-__global__ void __launch_bounds__(256) k_tiny(StepArgs a, Verts vs, S score) {
-  const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_tiny(StepArgs a, TierWork tw, S score) {
+  const int32_t mode = step_mode(a);
+  const int32_t nwork = tw.size(mode);
+  // grid-stride over whole warps so record_changes sees full warps
+  for (int32_t t0 = blockIdx.x * blockDim.x; t0 < nwork; t0 += gridDim.x * blockDim.x) {
+  const int32_t t = t0 + threadIdx.x;
   bool chg = false;
-  if (t < vs.n) {
-    const int32_t v = vs[t];
+  int32_t v = 0;
+  if (t < nwork) {
+    v = tw.at(mode, t);
     const int32_t b = a.off[v];
     const int32_t d = a.off[v + 1] - b;
     int32_t lab[TMAX];
@@ -140,7 +201,8 @@ __global__ void __launch_bounds__(256) k_tiny(StepArgs a, Verts vs, S score) {
     a.lout[v] = best.l;
     chg = best.l != a.lcur[v];
   }
-  warp_count_add(a.changed, chg);
+  record_changes(a, chg, v);
+  }
 }
 
 // --------------------------------------------------------------- group tier
@@ -148,23 +210,27 @@ __global__ void __launch_bounds__(256) k_tiny(StepArgs a, Verts vs, S score) {
 // vertices with all loads issued before any counting.  The match key carries
 // the group index so equal labels of different vertices do not merge.
 template <int G, int U, bool W, class S>
-__global__ void __launch_bounds__(256) k_group(StepArgs a, Verts vs, S score) {
+__global__ void __launch_bounds__(256) k_group(StepArgs a, TierWork tw, S score) {
   constexpr int PER = 32 / G;
+  const int32_t mode = step_mode(a);
+  const int32_t nwork = tw.size(mode);
   const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp * U * PER < nwork;
+       warp += nwarps) {
   int32_t v[U], lab[U];
   uint32_t wt[U];
   bool act[U], has[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     const int64_t grp = (warp * U + u) * PER + lane / G;
-    act[u] = grp < vs.n;
+    act[u] = grp < nwork;
     has[u] = false;
     v[u] = 0;
     wt[u] = 0;
     int32_t col = 0;
     if (act[u]) {
-      v[u] = vs[grp];
+      v[u] = tw.at(mode, grp);
       const int32_t b = a.off[v[u]], e = a.off[v[u] + 1];
       const int32_t j = b + (lane & (G - 1));
       has[u] = j < e;
@@ -186,12 +252,16 @@ __global__ void __launch_bounds__(256) k_group(StepArgs a, Verts vs, S score) {
     Best c = best_none();
     if (has[u] && lane == __ffs(m) - 1) c = Best{score(lab[u], k), lab[u]};
     c = group_max<G>(c);
-    if (act[u] && (lane & (G - 1)) == 0) {
+    const bool writer = act[u] && (lane & (G - 1)) == 0;
+    bool ch = false;
+    if (writer) {
       a.lout[v[u]] = c.l;
-      chg += c.l != a.lcur[v[u]];
+      ch = c.l != a.lcur[v[u]];
     }
+    record_changes(a, ch, v[u]);
   }
-  warp_count_add(a.changed, chg);
+  (void)chg;
+  }
 }
 
 // Count one 32-edge chunk: lanes with equal labels are merged by
@@ -220,26 +290,39 @@ __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, 
 template <bool W>
 __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_t mid_max, FailList fmid,
                                                     FailList fbig) {
+  constexpr int U = 8;  // column loads in flight per lane
   if (!use_majority(a)) return;
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  // the next vertex's offsets and label are fetched while this one streams
+  int32_t nv_b = 0, nv_e = 0, nv_c = 0, nv_v = 0;
+  if (gw < vs.n) {
+    nv_v = vs[gw];
+    nv_b = a.off[nv_v];
+    nv_e = a.off[nv_v + 1];
+    nv_c = a.lcur[nv_v];
+  }
   for (int64_t i = gw; i < vs.n; i += nw) {
-    const int32_t v = vs[i];
-    const int32_t b = a.off[v], e = a.off[v + 1];
-    const int32_t cand = a.lcur[v];
+    const int32_t v = nv_v, b = nv_b, e = nv_e, cand = nv_c;
+    if (i + nw < vs.n) {
+      nv_v = vs[i + nw];
+      nv_b = a.off[nv_v];
+      nv_e = a.off[nv_v + 1];
+      nv_c = a.lcur[nv_v];
+    }
     uint32_t cnt = 0, tot = 0;
-    for (int32_t j0 = b + lane; j0 < e; j0 += 128) {
-      int32_t c[4];
-      uint32_t wt[4];
+    for (int32_t j0 = b + lane; j0 < e; j0 += 32 * U) {
+      int32_t c[U];
+      uint32_t wt[U];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < U; ++q) {
         const int32_t j = j0 + 32 * q;
         c[q] = j < e ? ld_stream(a.cols + j) : -1;
         wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < U; ++q) {
         const int32_t l = c[q] >= 0 ? ld_label(a.lin + c[q]) : -1;
         cnt += l == cand ? wt[q] : 0u;
         tot += wt[q];
@@ -263,17 +346,17 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
 // sized to the power of two >= 2*degree; batches of 4 chunks of 32 edges are
 // loaded before they are counted.
 template <int CAP, int NT, bool W, class S>
-__global__ void __launch_bounds__(NT) k_mid(StepArgs a, Verts vs, FailList fl, S score) {
+__global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
   __shared__ uint32_t skeys[NW][CAP];
   __shared__ uint32_t svals[NW][CAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  bool listed;
-  const int32_t nwork = work_size(a, vs, fl, &listed);
+  const int32_t mode = step_mode(a);
+  const int32_t nwork = tw.size(mode);
   uint32_t* kk = skeys[warp];
   uint32_t* vv = svals[warp];
   for (int32_t i = blockIdx.x * NW + warp; i < nwork; i += gridDim.x * NW) {
-    const int32_t v = listed ? fl.ids[i] : vs[i];
+    const int32_t v = tw.at(mode, i);
     const int32_t b = a.off[v], e = a.off[v + 1];
     const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));
     for (uint32_t s = lane; s < cap; s += 32) {
@@ -304,12 +387,10 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, Verts vs, FailList fl, S
     }
     if (fail) atomicOr(a.err, kErrProbe);
     best = group_max<32>(best);
-    bool chg = false;
     if (lane == 0) {
       a.lout[v] = best.l;
-      chg = best.l != a.lcur[v];
+      if (best.l != a.lcur[v]) record_change(a, v);
     }
-    warp_count_add(a.changed, chg);
     __syncwarp();
   }
 }
@@ -318,14 +399,14 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, Verts vs, FailList fl, S
 // Exact count, one block per vertex (degree <= CAP/2): block shared table
 // (dynamic, CAP slots) sized per vertex to the power of two >= 2*degree.
 template <int NT, bool W, class S>
-__global__ void __launch_bounds__(NT) k_big(StepArgs a, Verts vs, FailList fl, S score) {
+__global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
   extern __shared__ uint32_t smem[];
   __shared__ Best red[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  bool listed;
-  const int32_t nwork = work_size(a, vs, fl, &listed);
+  const int32_t mode = step_mode(a);
+  const int32_t nwork = tw.size(mode);
   for (int32_t i = blockIdx.x; i < nwork; i += gridDim.x) {
-    const int32_t v = listed ? fl.ids[i] : vs[i];
+    const int32_t v = tw.at(mode, i);
     const int32_t b = a.off[v], e = a.off[v + 1];
     const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));
     uint32_t* keys = smem;
@@ -357,7 +438,7 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, Verts vs, FailList fl, S
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0) {
       a.lout[v] = best.l;
-      if (best.l != a.lcur[v]) atomicAdd(a.changed, 1ull);
+      if (best.l != a.lcur[v]) record_change(a, v);
     }
   }
 }
@@ -394,33 +475,34 @@ struct HubPlan {
   uint32_t* hub_state;           // [nhubs] 1 = decided by the majority pass this step
 };
 
-// Bucket of a key (high bits of one hash) and its table slot (another hash).
+// Bucket of a key: the high bits of its hash (table slots use the low bits).
 __device__ __forceinline__ uint32_t hub_bucket_of(uint32_t key, uint32_t nb) {
   return (uint32_t)(((unsigned long long)fmix32(key) * nb) >> 32);
 }
-__device__ __forceinline__ uint32_t hub_slot_of(uint32_t key) { return fmix32(key ^ 0x9e3779b9u); }
 
 template <int NT, bool W>
 __global__ void __launch_bounds__(NT) k_hub_majority(StepArgs a, HubPlan hp, int32_t nchunks) {
   __shared__ uint32_t red[2][NT / 32];
-  if (!use_majority(a)) return;
+  const int32_t mode = step_mode(a);
+  if (mode == kModeFull) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const int32_t h = hp.chunk_hub[c];
+    if (mode == kModeFrontier && hp.hub_state[h] != 2u) continue;  // block-uniform
     const int32_t cand = a.lcur[hp.hub_v[h]];
     const int32_t cb = hp.chunk_begin[c], ce = hp.chunk_end[c];
     uint32_t cnt = 0, tot = 0;
-    for (int32_t j0 = cb + threadIdx.x; j0 < ce; j0 += 4 * NT) {
-      int32_t col[4];
-      uint32_t wt[4];
+    for (int32_t j0 = cb + threadIdx.x; j0 < ce; j0 += 8 * NT) {
+      int32_t col[8];
+      uint32_t wt[8];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < 8; ++q) {
         const int32_t j = j0 + q * NT;
         col[q] = j < ce ? ld_stream(a.cols + j) : -1;
         wt[q] = j < ce ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < 8; ++q) {
         const int32_t l = col[q] >= 0 ? ld_label(a.lin + col[q]) : -1;
         cnt += l == cand ? wt[q] : 0u;
         tot += wt[q];
@@ -445,11 +527,15 @@ __global__ void __launch_bounds__(NT) k_hub_majority(StepArgs a, HubPlan hp, int
   }
 }
 
+// State after the step's majority pass: 1 = decided (or inactive), 0 = count
+// exactly.  In frontier mode only hubs marked active (state 2) take part.
 __global__ void k_hub_decide(StepArgs a, HubPlan hp) {
   const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= hp.nhubs) return;
+  const int32_t mode = step_mode(a);
+  if (mode == kModeFrontier && hp.hub_state[h] != 2u) return;  // inactive: keeps state 1
   bool major = false;
-  if (use_majority(a)) {
+  if (mode != kModeFull) {
     const unsigned long long p = hp.hub_cand[h];
     hp.hub_cand[h] = 0ull;
     const uint32_t kc = (uint32_t)(p >> 32), kt = (uint32_t)(p & 0xffffffffull);
@@ -495,44 +581,25 @@ __global__ void __launch_bounds__(NT) k_hub_bucket(StepArgs a, HubPlan hp, S sco
     __syncthreads();
     Best best = best_none();
     bool fail = false;
-    for (int32_t k0 = threadIdx.x; k0 < d; k0 += 4 * NT) {
+    auto ins = [&](uint32_t key, uint32_t k) {
+      return table_insert_bounded(keys, vals, kHubTable - 1, key, k, kHubTable, nullptr, nullptr);
+    };
+    // warp-uniform trip count: lanes of a warp read 32 consecutive labels
+    const int32_t warp_base = threadIdx.x & ~31;
+    for (int32_t k0 = warp_base; k0 < d; k0 += 4 * NT) {
       int32_t l[4];
       uint32_t wt[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int32_t k = k0 + q * NT;
+        const int32_t k = k0 + q * NT + (threadIdx.x & 31);
         l[q] = k < d ? __ldcg(lab + k) : -1;
         wt[q] = k < d ? (W ? (uint32_t)ld_stream(a.w + b + k) : 1u) : 0u;
+        // labels of other buckets take no part
+        if (l[q] >= 0 && nb > 1 && hub_bucket_of((uint32_t)l[q] + 1u, nb) != p) l[q] = -1;
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (l[q] < 0) continue;
-        const uint32_t key = (uint32_t)l[q] + 1u;
-        if (nb > 1 && hub_bucket_of(key, nb) != p) continue;
-        uint32_t sl = hub_slot_of(key) & (kHubTable - 1);
-        uint32_t tot = kNoSlot;
-        for (uint32_t probe = 0; probe < kHubTable; ++probe) {
-          const uint32_t kc = keys[sl];
-          if (kc == key) {
-            tot = atomicAdd(vals + sl, wt[q]) + wt[q];
-            break;
-          }
-          if (kc == 0) {
-            const uint32_t prev = atomicCAS(keys + sl, 0u, key);
-            if (prev == 0u || prev == key) {
-              tot = atomicAdd(vals + sl, wt[q]) + wt[q];
-              break;
-            }
-          }
-          sl = (sl + 1) & (kHubTable - 1);
-        }
-        if (tot == kNoSlot) {
-          fail = true;
-          continue;
-        }
-        const Best c{score(l[q], tot), l[q]};
-        if (better(c, best)) best = c;
-      }
+      for (int q = 0; q < 4; ++q)
+        if (k0 + q * NT < d) count_chunk<W>(l[q] >= 0, l[q], wt[q], score, ins, best, fail);
     }
     if (fail) atomicOr(a.err, kErrProbe);
     best = block_max<NT>(best, red);
@@ -551,7 +618,108 @@ __global__ void k_hub_finalize(StepArgs a, HubPlan hp) {
   const int32_t l = p ? (int32_t)(uint32_t)(p & 0xffffffffull) : a.lcur[v];
   if (!p) atomicOr(a.err, kErrHubPlan);
   a.lout[v] = l;
-  if (l != a.lcur[v]) atomicAdd(a.changed, 1ull);
+  if (l != a.lcur[v]) record_change(a, v);
+}
+
+// ----------------------------------------------------------- frontier mode
+// A vertex's new label is a function of its neighbours' labels; if none of
+// them changed in the previous step the result is its current label.  On a
+// symmetric CSR (every edge stored both ways) the vertices to recompute are
+// exactly the neighbours of the vertices that changed.  The previous step
+// listed its changed vertices (chg_in); marks carry this step's epoch, so
+// nothing is ever cleared.  The output buffer already holds the labels of
+// two steps back, which equal the current ones except for chg_in: those that
+// are not recomputed are copied.  No pass touches all n vertices.
+struct Frontier {
+  uint32_t* act;           // [n] epoch of the last step that marked the vertex
+  uint32_t epoch;          // this step's mark (unique per step of the handle)
+  const int32_t* chg_in;   // vertices changed in the previous step
+  const uint32_t* chg_in_n;
+  int32_t tiny_max, mid_max, big_max;
+  FailList tier[5];        // frontier members of tiny, g16, g32, mid, big
+};
+
+// One warp per changed vertex marks its neighbours; the first marker of a
+// vertex lists it in its tier (hubs are picked up by k_frontier_hubs).
+__global__ void __launch_bounds__(256) k_frontier_push(StepArgs a, Frontier f) {
+  if (step_mode(a) != kModeFrontier) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t nc = *f.chg_in_n;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nc; i += nw) {
+    const int32_t u = f.chg_in[i];
+    const int32_t b = a.off[u], e = a.off[u + 1];
+    for (int32_t j0 = b; j0 < e; j0 += 32) {
+      const int32_t j = j0 + lane;
+      int tier = -1;
+      int32_t x = 0;
+      if (j < e) {
+        x = ld_stream(a.cols + j);
+        if (atomicExch(f.act + x, f.epoch) != f.epoch) {
+          const int32_t d = a.off[x + 1] - a.off[x];
+          tier = d <= f.tiny_max ? 0 : d <= 16 ? 1 : d <= 32 ? 2 : d <= f.mid_max ? 3 : d <= f.big_max ? 4 : -1;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 5; ++t) {
+        const uint32_t m = __ballot_sync(kFull, tier == t);
+        if (!m) continue;
+        uint32_t base = 0;
+        if (lane == __ffs(m) - 1) base = atomicAdd(f.tier[t].count, (uint32_t)__popc(m));
+        base = __shfl_sync(kFull, base, __ffs(m) - 1);
+        if (tier == t) f.tier[t].ids[base + __popc(m & ((1u << lane) - 1u))] = x;
+      }
+    }
+  }
+}
+
+// Changed vertices that are not recomputed keep their (new) label.
+__global__ void __launch_bounds__(256) k_frontier_copy(StepArgs a, Frontier f) {
+  if (step_mode(a) != kModeFrontier) return;
+  const uint32_t nc = *f.chg_in_n;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = f.chg_in[i];
+    if (f.act[v] != f.epoch) a.lout[v] = a.lin[v];
+  }
+}
+
+// Marked hubs go through the majority check (state 2), unmarked ones are
+// done (state 1).
+__global__ void k_frontier_hubs(StepArgs a, Frontier f, HubPlan hp) {
+  if (step_mode(a) != kModeFrontier) return;
+  const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h < hp.nhubs) hp.hub_state[h] = f.act[hp.hub_v[h]] == f.epoch ? 2u : 1u;
+}
+
+// Symmetry check of a CSR with strictly ascending rows, one thread per edge:
+// every (v, u) needs (u, v).  bad |= 1 for an unsorted row, 2 for a missing
+// reverse edge.
+__global__ void k_check_symmetric(const int32_t* __restrict__ off, const int32_t* __restrict__ cols, int32_t n,
+                                  int64_t m, uint32_t* bad) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+    int32_t lo = 0, hi = n - 1;
+    while (lo < hi) {  // the row of edge j: last v with off[v] <= j
+      const int32_t mid = (int32_t)(((int64_t)lo + hi + 1) >> 1);
+      if (off[mid] <= j) lo = mid; else hi = mid - 1;
+    }
+    const int32_t v = lo, u = cols[j];
+    if (j > off[v] && cols[j - 1] >= u) {
+      atomicOr(bad, 1u);
+      continue;
+    }
+    int32_t a = off[u], b = off[u + 1] - 1;
+    bool found = false;
+    while (a <= b) {
+      const int32_t mid = (a + b) >> 1;
+      const int32_t x = cols[mid];
+      if (x == v) {
+        found = true;
+        break;
+      }
+      if (x < v) a = mid + 1; else b = mid - 1;
+    }
+    if (!found) atomicOr(bad, 2u);
+  }
 }
 
 // --------------------------------------------------------- layered volumes

@@ -107,9 +107,12 @@ class CSRGraph:
 class Graph:
     """A device-resident graph handle (glp_graph)."""
 
-    def __init__(self, g: CSR | CSRGraph):
+    def __init__(self, g: CSR | CSRGraph, symmetric: bool | None = None):
+        """`symmetric`: assert that every edge is stored both ways (default:
+        the CSR's own flag; otherwise the engine checks on the device)."""
         if isinstance(g, CSRGraph):
             g = g.csr()
+        sym = g.symmetric if symmetric is None else symmetric
         self._lib = _lib.load()
         self.n, self.m = g.n, g.m
         self.weighted = g.weights is not None
@@ -118,8 +121,9 @@ class Graph:
             torch.cuda.synchronize(g.device)
         h = C.c_void_p()
         w = C.c_void_p(g.weights.data_ptr()) if g.weights is not None else None
-        _lib.check(self._lib.glp_graph_create(C.c_void_p(g.offsets.data_ptr()), C.c_void_p(g.cols.data_ptr()), w,
-                                              g.n, C.c_int64(g.m), on_dev, C.byref(h)))
+        _lib.check(self._lib.glp_graph_create_ex(C.c_void_p(g.offsets.data_ptr()), C.c_void_p(g.cols.data_ptr()), w,
+                                                 g.n, C.c_int64(g.m), on_dev, _lib.GRAPH_SYMMETRIC if sym else 0,
+                                                 C.byref(h)))
         self._h = h
 
     def close(self) -> None:

@@ -34,6 +34,7 @@ class CSR:
     offsets: torch.Tensor
     cols: torch.Tensor
     weights: torch.Tensor | None = None
+    symmetric: bool = False  # every edge stored in both directions
 
     @property
     def n(self) -> int:
@@ -49,7 +50,7 @@ class CSR:
 
     def to(self, device) -> "CSR":
         w = self.weights.to(device) if self.weights is not None else None
-        return CSR(self.offsets.to(device), self.cols.to(device), w)
+        return CSR(self.offsets.to(device), self.cols.to(device), w, self.symmetric)
 
     def numpy(self):
         w = self.weights.cpu().numpy() if self.weights is not None else None
@@ -125,7 +126,7 @@ def build_csr(src: torch.Tensor, dst: torch.Tensor, n: int, relabel: bool = True
     cols = (keys & 0xFFFFFFFF).to(torch.int32)
     if int(offsets[-1].item()) >= 2**31:
         raise ValueError("graph exceeds int32 CSR")
-    return CSR(offsets.to(torch.int32), cols)
+    return CSR(offsets.to(torch.int32), cols, None, True)
 
 
 def add_weights(g: CSR, wmax: int = 16, seed: int = 1) -> CSR:
@@ -137,7 +138,7 @@ def add_weights(g: CSR, wmax: int = 16, seed: int = 1) -> CSR:
         torch.cuda.synchronize(g.device)
     _lib.check(lib.glp_edge_weights(C.c_void_p(_ptr(g.offsets)), C.c_void_p(_ptr(g.cols)), g.n, C.c_int64(g.m),
                                     wmax, C.c_uint64(seed), C.c_void_p(_ptr(w)), on_dev))
-    return CSR(g.offsets, g.cols, w)
+    return CSR(g.offsets, g.cols, w, g.symmetric)
 
 
 # ------------------------------------------------------------ workloads

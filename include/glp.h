@@ -126,6 +126,15 @@ int glp_params_default(glp_params* p);
  * in [0,n)); a malformed CSR returns GLP_EINVAL. */
 int glp_graph_create(const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n,
                      int64_t m, int32_t on_device, glp_graph** out);
+/* As glp_graph_create, with flags: GLP_GRAPH_SYMMETRIC asserts that every
+ * edge is stored in both directions (what CSRGraph builds for undirected
+ * input, header/graph.h:97-115), which lets converged classic steps
+ * recompute only the neighbours of changed vertices.  Without the flag the
+ * engine checks symmetry on the device the first time it could use it
+ * (rows must be strictly ascending to qualify). */
+#define GLP_GRAPH_SYMMETRIC 1u
+int glp_graph_create_ex(const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n,
+                        int64_t m, int32_t on_device, uint32_t flags, glp_graph** out);
 void glp_graph_destroy(glp_graph* g);
 int glp_graph_info(const glp_graph* g, int32_t* n, int64_t* m, int32_t* max_degree);
 /* Degree-tier plan for these params.  out[0..6]: vertices per tier

@@ -225,6 +225,29 @@ def test_device_resident_csr_input():
     np.testing.assert_array_equal(res.labels, O.classic_run(off, cols, 5))
 
 
+def test_directed_csr_without_frontier():
+    """A CSR that is not symmetric never takes the frontier shortcut."""
+    rng = np.random.default_rng(5)
+    n = 3000
+    adj = [sorted(set(rng.integers(0, n, size=rng.integers(1, 40)).tolist()) - {v}) for v in range(n)]
+    from tests.graphs_fixtures import csr_from_adj
+    off, cols = csr_from_adj(adj)
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, 12)
+    _, otr = O.classic_run(off, cols, 12, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+
+
+@pytest.mark.parametrize("case", ["rmat14", "planted20k", "two_cliques"])
+def test_classic_frontier_asserted_symmetric(case):
+    off, cols = CASES[case]
+    g = Graph(from_numpy(off, cols), symmetric=True)
+    trace = []
+    g.run(_lib.METHOD_CLASSIC, 15, callback=lambda it, lab: trace.append(lab) and False)
+    g.close()
+    _, otr = O.classic_run(off, cols, 15, trace=True)
+    np.testing.assert_array_equal(np.array(trace), otr)
+
+
 def test_malformed_csr_rejected():
     off = np.array([0, 2, 3], np.int32)
     cols = np.array([1, 5, 0], np.int32)  # 5 is out of range
