@@ -114,12 +114,16 @@ struct CountTable {
 };
 
 // Bounded insert: gives up after `max_probe` probes and returns kNoSlot.
-// Optionally appends newly claimed slots to `claimed` (count in *nclaimed).
+// Double hashing (odd stride from a second hash) avoids the long clustered
+// runs of linear probing, so the lanes of a warp finish their probes close
+// together.  Optionally appends newly claimed slots to `claimed`.
 constexpr uint32_t kNoSlot = 0xffffffffu;
 __device__ __forceinline__ uint32_t table_insert_bounded(uint32_t* keys, uint32_t* vals, uint32_t mask, uint32_t key,
                                                          uint32_t c, uint32_t max_probe, uint32_t* claimed,
                                                          uint32_t* nclaimed) {
-  uint32_t h = fmix32(key) & mask;
+  const uint32_t hk = fmix32(key);
+  uint32_t h = hk & mask;
+  const uint32_t step = (fmix32(hk ^ 0x5bd1e995u) | 1u) & mask;
   for (uint32_t probe = 0; probe < max_probe; ++probe) {
     const uint32_t cur = keys[h];
     if (cur == key) return atomicAdd(&vals[h], c) + c;
@@ -131,7 +135,7 @@ __device__ __forceinline__ uint32_t table_insert_bounded(uint32_t* keys, uint32_
       }
       if (prev == key) return atomicAdd(&vals[h], c) + c;
     }
-    h = (h + 1) & mask;
+    h = (h + (step ? step : 1u)) & mask;
   }
   return kNoSlot;
 }

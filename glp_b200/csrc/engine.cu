@@ -11,6 +11,7 @@
 //   run_slpa              <- SLPA loop (tutorial/Base5prop.cuh:264-293)
 #include <algorithm>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -78,7 +79,7 @@ int resolve_tiers(const glp_params* p, TierParams* t) {
   return GLP_OK;
 }
 
-// Degree tiers; hubs get ceil(deg / kHubBucket) hash buckets (one work item
+// Degree tiers; hubs get ceil(3*deg / kHubTable) hash buckets (one work item
 // each) and streaming chunks of hub_chunk edges.
 void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPlan* hp) {
   *hp = HostPlan{};
@@ -104,13 +105,16 @@ void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPla
     } else if (d <= t.big_max) {
       hp->big.push_back(v);
       hp->mb.push_back(v);
+      (d <= kBigSplit ? hp->big_lo : hp->big_hi).push_back(v);
       tier = 5;
     } else {
       tier = 6;
       const int32_t h = (int32_t)hp->hub_v.size();
-      const int32_t nb = (d + kHubBucket - 1) / kHubBucket;
+      const int32_t nb = (int32_t)((3ll * d + kHubTable - 1) / kHubTable);
       hp->hub_v.push_back(v);
       hp->hub_nb.push_back(nb);
+      hp->hub_item0.push_back((int32_t)hp->item_hub.size());
+      hp->max_nb = std::max(hp->max_nb, nb);
       hp->hub_lbase.push_back(hp->hub_labels);
       hp->hub_labels += d;
       for (int32_t b = 0; b < nb; ++b) {
@@ -184,6 +188,7 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
       (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
       (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
+      (rc = upload_verts(&p, hp.big_lo, &p.big_lo)) || (rc = upload_verts(&p, hp.big_hi, &p.big_hi)) ||
       (rc = zeroed(&p, 9, &p.counts)) || (rc = zeroed(&p, std::max<size_t>(hp.mid.size(), 1), &p.fmid.ids)) ||
       (rc = zeroed(&p, std::max<size_t>(hp.big.size(), 1), &p.fbig.ids)) || (rc = zeroed(&p, 1, &p.d_mode)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.front.act)) ||
@@ -219,13 +224,25 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
         (rc = upload(&p, hp.hub_nb, (int32_t**)&h.hub_nb)) ||
         (rc = upload(&p, hp.item_hub, (int32_t**)&h.item_hub)) ||
         (rc = upload(&p, hp.item_bucket, (int32_t**)&h.item_bucket)) ||
-        (rc = zeroed(&p, (size_t)hp.hub_labels, &h.hlab)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_best)) ||
+        (rc = upload(&p, hp.hub_item0, (int32_t**)&h.hub_item0)) ||
+        (rc = zeroed(&p, (size_t)hp.hub_labels, &h.hlab)) || (rc = zeroed(&p, (size_t)hp.hub_labels, &h.hsort)) ||
+        (rc = zeroed(&p, hp.item_hub.size(), &h.bcnt)) || (rc = zeroed(&p, hp.item_hub.size(), &h.bstart)) ||
+        (rc = zeroed(&p, hp.item_hub.size(), &h.bcur)) ||
+        (g->d_w && ((rc = zeroed(&p, (size_t)hp.hub_labels, &h.hw)) ||
+                    (rc = zeroed(&p, (size_t)hp.hub_labels, &h.hsw)))) ||
+        (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_best)) ||
         (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_cand)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_state))) {
       free_plan(&p);
       return rc;
     }
     h.nhubs = p.n_hubs;
     h.nitems = (int32_t)hp.item_hub.size();
+    h.max_nb = hp.max_nb;
+    if (hp.max_nb > 25600) {
+      free_plan(&p);
+      set_error("a vertex of degree above %d is not supported", 25600 / 3 * kHubTable);
+      return GLP_ENOTSUP;
+    }
   }
   p.valid = true;
   return GLP_OK;
@@ -241,8 +258,19 @@ static int allow_smem(K kernel, size_t bytes) {
 
 static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// GLP_SERIAL_STEP=1 keeps every kernel of a step on one stream (profiling).
+static bool serial_step() {
+  static const bool on = [] {
+    const char* e = std::getenv("GLP_SERIAL_STEP");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 template <bool W, class S>
-int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t* launches) {
+int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_t* launches) {
+  StepLaunch L = Lin;
+  if (serial_step()) L.aux[0] = L.aux[1] = L.stream;
   const DevicePlan& p = *L.plan;
   cudaStream_t s = L.stream;
   auto mark_on = [&](cudaStream_t st, int i, int which) -> int {
@@ -269,17 +297,20 @@ int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t*
     }
   }
   auto work = [&](const Verts& all, int k, const FailList* major) {
-    TierWork tw{all, major ? *major : FailList{nullptr, nullptr}, p.front.tier[k]};
+    TierWork tw{all, major ? *major : FailList{nullptr, nullptr}, p.front.tier[k], 0};
     return tw;
   };
   // fork: hubs on aux[0], the small tiers on aux[1], the rest here
   GLP_CUDA(cudaEventRecord(L.fork, s));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[0], L.fork, 0));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[1], L.fork, 0));
-  constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 1024, kGroupU = 4;
+  constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 512, kGroupU = 4;
   if (p.n_hubs) {
     const size_t sm = 2ull * kHubTable * sizeof(uint32_t);
-    if ((rc = allow_smem(k_hub_bucket<kBucketNT, W, S>, sm))) return rc;
+    const size_t sm_hist = (size_t)p.hub.max_nb * sizeof(uint32_t);
+    if ((rc = allow_smem(k_hub_bucket<kBucketNT, W, S>, sm)) || (rc = allow_smem(k_hub_gather<kHubNT, W>, sm_hist)) ||
+        (rc = allow_smem(k_hub_scatter<kHubNT, W>, 2 * sm_hist)))
+      return rc;
     if ((rc = mark_on(L.aux[0], 5, 0))) return rc;
     const unsigned grid = (unsigned)std::min<int64_t>(p.n_chunks, kMaxGrid);
     const unsigned hgrid = (unsigned)cdiv(p.n_hubs, 256);
@@ -288,11 +319,14 @@ int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t*
       ++*launches;
     }
     k_hub_decide<<<hgrid, 256, 0, L.aux[0]>>>(a, p.hub);
-    k_hub_gather<kHubNT><<<grid, kHubNT, 0, L.aux[0]>>>(a, p.hub, p.n_chunks);
-    k_hub_bucket<kBucketNT, W, S><<<(unsigned)std::min<int64_t>(p.hub.nitems, 148 * 4), kBucketNT, sm, L.aux[0]>>>(
+    GLP_CUDA(cudaMemsetAsync(p.hub.bcnt, 0, sizeof(uint32_t) * p.hub.nitems, L.aux[0]));
+    k_hub_gather<kHubNT, W><<<grid, kHubNT, sm_hist, L.aux[0]>>>(a, p.hub, p.n_chunks);
+    k_hub_offsets<<<hgrid, 256, 0, L.aux[0]>>>(p.hub);
+    k_hub_scatter<kHubNT, W><<<grid, kHubNT, 2 * sm_hist, L.aux[0]>>>(a, p.hub, p.n_chunks);
+    k_hub_bucket<kBucketNT, W, S><<<(unsigned)std::min<int64_t>(p.hub.nitems, 148 * 8), kBucketNT, sm, L.aux[0]>>>(
         a, p.hub, score);
     k_hub_finalize<<<hgrid, 256, 0, L.aux[0]>>>(a, p.hub);
-    *launches += 4;
+    *launches += 6;
     if ((rc = mark_on(L.aux[0], 5, 1))) return rc;
   }
   if (L.allow_majority && modal && p.mb.n) {
@@ -303,11 +337,23 @@ int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t*
     ++*launches;
   }
   if (p.big.n) {
+    // full mode: degrees <= kBigSplit in small-table blocks, the rest with the
+    // full table; majority and frontier lists all go to the full-table launch
+    const size_t sm_lo = 4ull * kBigSplit * sizeof(uint32_t);
     const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
     if ((rc = allow_smem(k_big<kBigNT, W, S>, sm))) return rc;
     if ((rc = mark_on(s, 4, 0))) return rc;
-    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, work(p.big, 4, &p.fbig),
-                                                                                          score);
+    if (p.big_lo.n) {
+      TierWork lo{p.big_lo, FailList{nullptr, nullptr}, FailList{nullptr, nullptr}, 1};
+      k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big_lo.n, kMaxGrid), kBigNT, sm_lo, s>>>(a, lo, score);
+      ++*launches;
+    }
+    TierWork hi = work(p.big_hi, 4, &p.fbig);
+    hi.front = p.front.tier[4];
+    // outside full mode this launch takes the whole tier's lists
+    const bool any_hi = p.big_hi.n > 0;
+    if (!any_hi) hi.all = Verts{nullptr, 0, 0};
+    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, hi, score);
     if ((rc = mark_on(s, 4, 1))) return rc;
     ++*launches;
   }
@@ -321,7 +367,8 @@ int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t*
   if (p.g32.n) {
     if ((rc = mark_on(L.aux[1], 2, 0))) return rc;
     const int64_t warps = cdiv(p.g32.n, 1 * kGroupU);
-    k_group<32, kGroupU, W, S><<<(unsigned)std::min<int64_t>(cdiv(warps * 32, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
+    (void)warps;
+    k_tiny<32, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.g32.n, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
         a, work(p.g32, 2, nullptr), score);
     if ((rc = mark_on(L.aux[1], 2, 1))) return rc;
     ++*launches;
@@ -329,7 +376,8 @@ int launch_step(const StepLaunch& L, const StepArgs& a, const S& score, int64_t*
   if (p.g16.n) {
     if ((rc = mark_on(L.aux[1], 1, 0))) return rc;
     const int64_t warps = cdiv(p.g16.n, 2 * kGroupU);
-    k_group<16, kGroupU, W, S><<<(unsigned)std::min<int64_t>(cdiv(warps * 32, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
+    (void)warps;
+    k_tiny<16, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.g16.n, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
         a, work(p.g16, 1, nullptr), score);
     if ((rc = mark_on(L.aux[1], 1, 1))) return rc;
     ++*launches;
@@ -502,6 +550,37 @@ static int init_labels(RunCtx& c) {
   return GLP_OK;
 }
 
+// Decides (once per handle) whether every row is strictly ascending.
+static int ensure_sorted(glp_graph* g) {
+  if (g->rows_sorted >= 0) return GLP_OK;
+  if (g->m == 0) {
+    g->rows_sorted = 1;
+    return GLP_OK;
+  }
+  uint32_t* d_bad = nullptr;
+  GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
+  GLP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), g->stream));
+  k_check_sorted<<<148 * 16, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, d_bad);
+  uint32_t bad = 1;
+  GLP_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, g->stream));
+  GLP_CUDA(cudaStreamSynchronize(g->stream));
+  cudaFree(d_bad);
+  g->rows_sorted = bad == 0 ? 1 : 0;
+  return GLP_OK;
+}
+
+// Exact first step when the labels are the vertex ids and rows are strictly
+// ascending (k_first_step), timed as a step.
+static int first_step(RunCtx& c, const StepArgs& a) {
+  StepLaunch L = c.launch();
+  if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[16], c.s));
+  k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), 148 * 32), 256, 0, c.s>>>(a);
+  ++c.launches;
+  GLP_CUDA(cudaGetLastError());
+  if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[17], c.s));
+  return GLP_OK;
+}
+
 // Decides (once per handle) whether the CSR stores every edge both ways.
 static int ensure_symmetric(glp_graph* g) {
   if (g->symmetric >= 0) return GLP_OK;
@@ -544,7 +623,15 @@ static int run_classic(RunCtx& c, int32_t niter) {
       L.front.chg_in = p.chg[(it - 1) & 1];
       L.front.chg_in_n = p.counts + 7 + ((it - 1) & 1);
     }
-    if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) return rc;
+    if (it == 0 && !W && g->rows_sorted == 1) {
+      if (c.timing) {  // first_step takes the step's events itself
+        c.used--;
+        c.ran.pop_back();
+      }
+      if ((rc = first_step(c, a))) return rc;
+    } else if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) {
+      return rc;
+    }
     if ((rc = after_iter(c, it, g->d_lab[(it + 1) & 1]))) return rc;
   }
   return GLP_OK;
@@ -614,7 +701,16 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
                g->plan.d_mode, g->n, nullptr, nullptr};
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
     L.allow_majority = 1;  // the listener mode; spoken labels change every step: no frontier
-    if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) return rc;
+    if (it == 0 && !W && g->rows_sorted == 1) {
+      // the step's events were taken by c.launch() above; the first step records them
+      if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[16], c.s));
+      k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), 148 * 32), 256, 0, c.s>>>(a);
+      ++c.launches;
+      GLP_CUDA(cudaGetLastError());
+      if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[17], c.s));
+    } else if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) {
+      return rc;
+    }
     if ((rc = after_iter(c, it, lout))) return rc;
   }
   if (out->slpa_comm && g->n) {
@@ -1011,6 +1107,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;
+  if ((method == GLP_METHOD_CLASSIC || method == GLP_METHOD_SLPA) && (rc = ensure_sorted(g))) return rc;
   if (method == GLP_METHOD_CLASSIC && (rc = ensure_symmetric(g))) return rc;
   switch (method) {
     case GLP_METHOD_CLASSIC:

@@ -23,6 +23,9 @@ int cuda_fail(cudaError_t e, const char* what);
 // Exact-count tier limits: a mid warp's table holds kMidCap slots, a big
 // block's table kBigCap slots (both at most half full).
 constexpr int kMidCap = 512, kBigCap = 8192;
+// In full mode big vertices up to kBigSplit degrees use a block with a table
+// of 2*kBigSplit slots (more blocks per SM); the rest of the tier the full one.
+constexpr int kBigSplit = 1024;
 
 struct TierParams {
   int32_t tiny_max = 8;       // <= 8
@@ -38,10 +41,12 @@ int resolve_tiers(const glp_params* p, TierParams* t);
 // Host-side plan (pure function of the offsets and the tier parameters).
 struct HostPlan {
   std::vector<int32_t> tiny, g16, g32, mid, big, mb;  // vertex lists (ascending ids); mb = mid + big
+  std::vector<int32_t> big_lo, big_hi;                 // the big tier split at kBigSplit
   int64_t isolated = 0;
   int64_t edges[7] = {0, 0, 0, 0, 0, 0, 0};  // per tier, as the vertex counts of glp_graph_plan
   // hubs
-  std::vector<int32_t> hub_v, hub_nb;
+  std::vector<int32_t> hub_v, hub_nb, hub_item0;
+  int32_t max_nb = 0;
   std::vector<int64_t> hub_lbase;
   std::vector<int32_t> chunk_hub, chunk_begin, chunk_end;
   std::vector<int32_t> item_hub, item_bucket;
@@ -52,7 +57,7 @@ void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPla
 struct DevicePlan {
   TierParams tiers;
   bool valid = false;
-  Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{};
+  Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{}, big_lo{}, big_hi{};
   FailList fmid{}, fbig{};
   // list counters: [majority mid, majority big, frontier tiny, g16, g32, mid,
   // big] are zeroed at the start of every step; [7 + s] counts the changed
@@ -111,7 +116,8 @@ struct glp_graph {
   // method-4 spill tables (2 slots per CSR entry), allocated on first use
   uint32_t* d_hook_keys = nullptr;
   double* d_hook_vals = nullptr;
-  int symmetric = -1;  // -1 unknown, 0 no, 1 yes (every edge stored both ways)
+  int symmetric = -1;    // -1 unknown, 0 no, 1 yes (every edge stored both ways)
+  int rows_sorted = -1;  // -1 unknown, 0 no, 1 every row strictly ascending
   uint32_t epoch = 0;  // frontier mark of the last step
   // auxiliary streams and fork/join events of a step
   cudaStream_t aux[2] = {nullptr, nullptr};

@@ -13,7 +13,7 @@
 //   group (9..32)      : 16 or 32 lanes per vertex, one __match_any_sync round
 //   mid   (33..256)    : one warp per vertex, per-warp shared-memory table
 //   big   (257..4096)  : one block per vertex, block shared-memory table
-//   hub   (> 4096)     : labels gathered once, then counted per hash bucket,
+//   hub   (> 4096)     : labels gathered once and sorted into hash buckets,
 //                        one block per (hub, bucket) with a shared table
 // Majority shortcut (classic, weighted, SLPA listener): when a vertex's own
 // label holds more than half of its neighbourhood weight it is the unique
@@ -116,7 +116,9 @@ struct TierWork {
   Verts all;
   FailList major;  // ids == nullptr: the tier has no pre-pass
   FailList front;
+  int full_only;   // 1: works only in full mode (a sub-range of a tier)
   __device__ __forceinline__ int32_t size(int32_t mode) const {
+    if (full_only) return mode == kModeFull ? all.n : 0;
     if (mode == kModeFrontier && front.ids) return (int32_t)*front.count;
     if (mode == kModeMajority && major.ids) return (int32_t)*major.count;
     return all.n;
@@ -264,22 +266,32 @@ __global__ void __launch_bounds__(256) k_group(StepArgs a, TierWork tw, S score)
   }
 }
 
-// Count one 32-edge chunk: lanes with equal labels are merged by
-// __match_any_sync and their leader adds the group's count to the table.
+// Count one 32-edge chunk: every lane adds its own label to the table and
+// keeps the best (score, label) of the running totals it saw.  Lanes holding
+// lane 0's label add once, through lane 0 (a hot label of a forming
+// community costs one atomic per warp).  Other lanes are not merged:
+// __match_any_sync costs a round per distinct value on B200, while a 32-bit
+// shared atomicAdd stays cheap under moderate contention.  Called by all
+// lanes of the warp.
 template <bool W, class S, class Ins>
 __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, const S& score, const Ins& insert,
                                             Best& best, bool& fail) {
   const int lane = threadIdx.x & 31;
-  const uint32_t m = __match_any_sync(kFull, (uint32_t)lab);
-  const uint32_t k = W ? __reduce_add_sync(m, wt) : (uint32_t)__popc(m);
-  if (has && lane == __ffs(m) - 1) {
-    const uint32_t tot = insert((uint32_t)lab + 1u, k);
-    if (tot == kNoSlot) {
-      fail = true;
-    } else {
-      const Best c{score(lab, tot), lab};
-      if (better(c, best)) best = c;
-    }
+  const int32_t l0 = __shfl_sync(kFull, has ? lab : -1, 0);
+  const uint32_t m0 = __ballot_sync(kFull, has && lab == l0);
+  uint32_t k = W ? wt : 1u;
+  if (l0 >= 0) {
+    const uint32_t k0 = W ? __reduce_add_sync(kFull, lab == l0 && has ? wt : 0u) : (uint32_t)__popc(m0);
+    if (lane == 0) k = k0;
+    else if (has && lab == l0) has = false;  // counted by lane 0
+  }
+  if (!has) return;
+  const uint32_t tot = insert((uint32_t)lab + 1u, k);
+  if (tot == kNoSlot) {
+    fail = true;
+  } else {
+    const Best c{score(lab, tot), lab};
+    if (better(c, best)) best = c;
   }
 }
 
@@ -400,7 +412,7 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
 // (dynamic, CAP slots) sized per vertex to the power of two >= 2*degree.
 template <int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
-  extern __shared__ uint32_t smem[];
+  extern __shared__ __align__(8) uint32_t smem[];
   __shared__ Best red[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
@@ -444,20 +456,22 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
 }
 
 // ----------------------------------------------------------------- hub tier
-// Vertices above the big tier.  Each hub h has P_h hash buckets (about
-// kHubBucket labels each).  Every pass is its own launch; no block waits on
-// another:
+// Vertices above the big tier.  Hub h gets nb_h = ceil(3*deg/kHubTable) hash
+// buckets, so a bucket averages at most kHubTable/3 labels and its distinct
+// labels fit a shared table of kHubTable slots at most half full.  Every
+// pass is its own launch; no block waits on another:
 //   k_hub_majority : chunks add (own-label weight, total weight) per hub;
 //   k_hub_decide   : a strict majority decides the hub (state 1);
-//   k_hub_gather   : chunks of undecided hubs gather their labels into a
-//                    compact scratch array (one random gather per edge);
-//   k_hub_bucket   : one block per (hub, bucket) streams the hub's gathered
-//                    labels, counts those hashing to its bucket in a shared
-//                    table (at most twice the expected size), and folds its
-//                    (score, label) maximum into the hub's best;
+//   k_hub_gather   : chunks of undecided hubs gather their labels (one random
+//                    gather per edge) and count them per bucket;
+//   k_hub_offsets  : per hub, bucket counts -> bucket starts (and cursors);
+//   k_hub_scatter  : chunks place their labels bucket-contiguously;
+//   k_hub_bucket   : one block per (hub, bucket) counts its own labels in a
+//                    shared table and folds its (score, label) maximum into
+//                    the hub's best (a bucket too large for the table is
+//                    counted in exact hashed sub-passes);
 //   k_hub_finalize : undecided hubs take their best label.
-constexpr int kHubBucket = 8192;           // target labels per bucket
-constexpr int kHubTable = 2 * kHubBucket;  // shared slots per bucket block
+constexpr int kHubTable = 8192;  // shared slots per bucket block
 
 struct HubPlan {
   const int32_t* chunk_hub;    // [nchunks] hub index of each chunk
@@ -466,10 +480,17 @@ struct HubPlan {
   const int32_t* hub_v;        // [nhubs] vertex id
   const int64_t* hub_lbase;    // [nhubs] first entry of the hub in the label scratch
   const int32_t* hub_nb;       // [nhubs] hash buckets
+  const int32_t* hub_item0;    // [nhubs] first (hub, bucket) item of the hub
   const int32_t* item_hub;     // [nitems] (hub, bucket) work items
   const int32_t* item_bucket;
-  int32_t* hlab;               // gathered labels of undecided hubs
-  int32_t nhubs, nitems;
+  int32_t* hlab;               // [labels] gathered labels (edge order)
+  int32_t* hsort;              // [labels] labels in bucket order
+  int32_t* hw;                 // [labels] weights in edge order (weighted graphs)
+  int32_t* hsw;                // [labels] weights in bucket order (weighted graphs)
+  uint32_t* bcnt;              // [nitems] labels per bucket
+  uint32_t* bstart;            // [nitems] bucket start (relative to the hub)
+  uint32_t* bcur;              // [nitems] scatter cursor
+  int32_t nhubs, nitems, max_nb;
   unsigned long long* hub_best;  // [nhubs] packed best (0 = none)
   unsigned long long* hub_cand;  // [nhubs] (own-label weight << 32) + total weight
   uint32_t* hub_state;           // [nhubs] 1 = decided by the majority pass this step
@@ -546,62 +567,147 @@ __global__ void k_hub_decide(StepArgs a, HubPlan hp) {
   hp.hub_state[h] = major ? 1u : 0u;
 }
 
-template <int NT>
+// Gathers the labels of undecided hubs and counts them per bucket
+// (block-local histogram, one global add per nonzero bucket).
+template <int NT, bool W>
 __global__ void __launch_bounds__(NT) k_hub_gather(StepArgs a, HubPlan hp, int32_t nchunks) {
+  extern __shared__ uint32_t hist[];  // [max_nb]
   for (int32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const int32_t h = hp.chunk_hub[c];
     if (hp.hub_state[h]) continue;  // block-uniform
+    const uint32_t nb = (uint32_t)hp.hub_nb[h];
     const int32_t cb = hp.chunk_begin[c], ce = hp.chunk_end[c];
     const int64_t base = hp.hub_lbase[h] - a.off[hp.hub_v[h]];
+    for (uint32_t b = threadIdx.x; b < nb; b += NT) hist[b] = 0;
+    __syncthreads();
     for (int32_t j0 = cb + threadIdx.x; j0 < ce; j0 += 4 * NT) {
       int32_t col[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) col[q] = j0 + q * NT < ce ? ld_stream(a.cols + j0 + q * NT) : -1;
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (col[q] >= 0) hp.hlab[base + j0 + q * NT] = ld_label(a.lin + col[q]);
+      for (int q = 0; q < 4; ++q) {
+        if (col[q] < 0) continue;
+        const int32_t j = j0 + q * NT;
+        const int32_t l = ld_label(a.lin + col[q]);
+        hp.hlab[base + j] = l;
+        if (W) hp.hw[base + j] = ld_stream(a.w + j);
+        atomicAdd(hist + (nb > 1 ? hub_bucket_of((uint32_t)l + 1u, nb) : 0u), 1u);
+      }
     }
+    __syncthreads();
+    const int32_t item0 = hp.hub_item0[h];
+    for (uint32_t b = threadIdx.x; b < nb; b += NT)
+      if (hist[b]) atomicAdd(hp.bcnt + item0 + b, hist[b]);
+    __syncthreads();
   }
 }
 
+// Bucket starts from the counts (exclusive scan per hub); counts stay.
+__global__ void k_hub_offsets(HubPlan hp) {
+  const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= hp.nhubs || hp.hub_state[h]) return;
+  const int32_t item0 = hp.hub_item0[h], nb = hp.hub_nb[h];
+  uint32_t run = 0;
+  for (int32_t b = 0; b < nb; ++b) {
+    hp.bstart[item0 + b] = run;
+    hp.bcur[item0 + b] = run;
+    run += hp.bcnt[item0 + b];
+  }
+}
+
+// Places the gathered labels bucket-contiguously: a block counts its labels
+// per bucket, reserves each bucket's range with one global add, then every
+// label takes a slot of its bucket's range.
+template <int NT, bool W>
+__global__ void __launch_bounds__(NT) k_hub_scatter(StepArgs a, HubPlan hp, int32_t nchunks) {
+  extern __shared__ uint32_t sh[];  // [max_nb] counts, then [max_nb] cursors
+  uint32_t* cnt = sh;
+  uint32_t* cur = sh + hp.max_nb;
+  for (int32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const int32_t h = hp.chunk_hub[c];
+    if (hp.hub_state[h]) continue;  // block-uniform
+    const uint32_t nb = (uint32_t)hp.hub_nb[h];
+    const int32_t cb = hp.chunk_begin[c], ce = hp.chunk_end[c];
+    const int64_t lb = hp.hub_lbase[h];
+    const int64_t base = lb - a.off[hp.hub_v[h]];
+    const int32_t item0 = hp.hub_item0[h];
+    for (uint32_t b = threadIdx.x; b < nb; b += NT) cnt[b] = 0;
+    __syncthreads();
+    for (int32_t j = cb + threadIdx.x; j < ce; j += NT) {
+      const int32_t l = hp.hlab[base + j];
+      atomicAdd(cnt + (nb > 1 ? hub_bucket_of((uint32_t)l + 1u, nb) : 0u), 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < nb; b += NT) cur[b] = cnt[b] ? atomicAdd(hp.bcur + item0 + b, cnt[b]) : 0u;
+    __syncthreads();
+    for (int32_t j = cb + threadIdx.x; j < ce; j += NT) {
+      const int32_t l = hp.hlab[base + j];
+      const uint32_t b = nb > 1 ? hub_bucket_of((uint32_t)l + 1u, nb) : 0u;
+      const uint32_t pos = atomicAdd(cur + b, 1u);
+      hp.hsort[lb + pos] = l;
+      if (W) hp.hsw[lb + pos] = hp.hw[base + j];
+    }
+    __syncthreads();
+  }
+}
+
+// One block per (hub, bucket): exact count of the bucket's labels in one
+// pass; if its distinct labels overflow the table (an insert gives up after
+// kHubProbe probes), the bucket is recounted in 2, 4, ... hashed sub-passes.
+constexpr uint32_t kHubProbe = 64;
+
 template <int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_hub_bucket(StepArgs a, HubPlan hp, S score) {
-  extern __shared__ uint32_t smem[];
-  uint32_t* keys = smem;
-  uint32_t* vals = smem + kHubTable;
+  extern __shared__ uint32_t hsm[];
   __shared__ Best red[32];
+  __shared__ int overflow;
   for (int32_t it = blockIdx.x; it < hp.nitems; it += gridDim.x) {
     const int32_t h = hp.item_hub[it];
     if (hp.hub_state[h]) continue;  // block-uniform
-    const uint32_t p = (uint32_t)hp.item_bucket[it], nb = (uint32_t)hp.hub_nb[h];
-    const int32_t v = hp.hub_v[h];
-    const int32_t b = a.off[v], d = a.off[v + 1] - b;
-    const int32_t* lab = hp.hlab + hp.hub_lbase[h];
-    for (uint32_t s = threadIdx.x; s < 2 * kHubTable; s += NT) smem[s] = 0;
-    __syncthreads();
+    const uint32_t size = hp.bcnt[it];
+    const int64_t beg = hp.hub_lbase[h] + hp.bstart[it];
     Best best = best_none();
-    bool fail = false;
-    auto ins = [&](uint32_t key, uint32_t k) {
-      return table_insert_bounded(keys, vals, kHubTable - 1, key, k, kHubTable, nullptr, nullptr);
-    };
-    // warp-uniform trip count: lanes of a warp read 32 consecutive labels
-    const int32_t warp_base = threadIdx.x & ~31;
-    for (int32_t k0 = warp_base; k0 < d; k0 += 4 * NT) {
-      int32_t l[4];
-      uint32_t wt[4];
+    for (uint32_t nsub = 1;; nsub *= 2) {
+      best = best_none();
+      if (threadIdx.x == 0) overflow = 0;
+      const uint32_t cap = nsub > 1 ? (uint32_t)kHubTable
+                                    : (size * 2u < (uint32_t)kHubTable ? pow2_ceil(2u * (size ? size : 1u))
+                                                                        : (uint32_t)kHubTable);
+      for (uint32_t sub = 0; sub < nsub; ++sub) {
+        uint32_t* keys = hsm;
+        uint32_t* vals = hsm + cap;
+        for (uint32_t s = threadIdx.x; s < 2 * cap; s += NT) hsm[s] = 0;
+        __syncthreads();
+        bool fail = false;
+        auto ins = [&](uint32_t key, uint32_t k) {
+          return table_insert_bounded(keys, vals, cap - 1, key, k, kHubProbe, nullptr, nullptr);
+        };
+        // warp-uniform trip count: the lanes of a warp read 32 consecutive labels
+        for (uint32_t k0 = threadIdx.x & ~31u; k0 < size; k0 += 4 * NT) {
+          int32_t l[4];
+          uint32_t wt[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int32_t k = k0 + q * NT + (threadIdx.x & 31);
-        l[q] = k < d ? __ldcg(lab + k) : -1;
-        wt[q] = k < d ? (W ? (uint32_t)ld_stream(a.w + b + k) : 1u) : 0u;
-        // labels of other buckets take no part
-        if (l[q] >= 0 && nb > 1 && hub_bucket_of((uint32_t)l[q] + 1u, nb) != p) l[q] = -1;
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t k = k0 + q * NT + (threadIdx.x & 31);
+            l[q] = k < size ? __ldcg(hp.hsort + beg + k) : -1;
+            wt[q] = k < size ? (W ? (uint32_t)__ldcg(hp.hsw + beg + k) : 1u) : 0u;
+            // sub-pass filter: another hash of the key (bucket bits are high bits)
+            if (nsub > 1 && l[q] >= 0 && (fmix32(((uint32_t)l[q] + 1u) ^ 0x2545f491u) & (nsub - 1)) != sub) l[q] = -1;
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (k0 + q * NT < size) count_chunk<W>(l[q] >= 0, l[q], wt[q], score, ins, best, fail);
+        }
+        if (fail) overflow = 1;
+        __syncthreads();
+        if (overflow) break;  // block-uniform
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (k0 + q * NT < d) count_chunk<W>(l[q] >= 0, l[q], wt[q], score, ins, best, fail);
+      if (!overflow) break;
+      if (nsub >= 1024u) {  // cannot happen for int32 sizes; stop rather than loop
+        if (threadIdx.x == 0) atomicOr(a.err, kErrProbe);
+        break;
+      }
     }
-    if (fail) atomicOr(a.err, kErrProbe);
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0 && best.l >= 0) atomicMax(hp.hub_best + h, pack_best(best, a.err));
     __syncthreads();
@@ -619,6 +725,41 @@ __global__ void k_hub_finalize(StepArgs a, HubPlan hp) {
   if (!p) atomicOr(a.err, kErrHubPlan);
   a.lout[v] = l;
   if (l != a.lcur[v]) record_change(a, v);
+}
+
+// ------------------------------------------------------- first-step shortcut
+// Before the first step every label is its vertex id.  When every row lists
+// strictly ascending columns (no repeated neighbour), every neighbour label
+// occurs once, so all counts are 1 and the tie rule picks the largest label:
+// the row's last column.  Exact for classic LP and the SLPA listener
+// (unweighted).
+__global__ void __launch_bounds__(256) k_first_step(StepArgs a) {
+  for (int32_t v0 = blockIdx.x * blockDim.x; v0 < a.n; v0 += gridDim.x * blockDim.x) {
+    const int32_t v = v0 + threadIdx.x;
+    bool chg = false;
+    if (v < a.n) {
+      const int32_t e = a.off[v + 1];
+      if (e > a.off[v]) {
+        const int32_t l = a.lin[a.cols[e - 1]];
+        a.lout[v] = l;
+        chg = l != a.lcur[v];
+      }
+    }
+    record_changes(a, chg, v);
+  }
+}
+
+// bad |= 1 when some row is not strictly ascending.
+__global__ void k_check_sorted(const int32_t* __restrict__ off, const int32_t* __restrict__ cols, int32_t n,
+                               uint32_t* bad) {
+  for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const int32_t b = off[v], e = off[v + 1];
+    for (int32_t j = b + 1; j < e; ++j)
+      if (cols[j - 1] >= cols[j]) {
+        atomicOr(bad, 1u);
+        break;
+      }
+  }
 }
 
 // ----------------------------------------------------------- frontier mode
@@ -724,11 +865,16 @@ __global__ void k_check_symmetric(const int32_t* __restrict__ off, const int32_t
 
 // --------------------------------------------------------- layered volumes
 // vol[l] += #vertices whose label is l (warp-aggregated atomics).
+// Lanes holding lane 0's label add once for all (hot labels of converged
+// communities); the others add directly.
 __global__ void __launch_bounds__(256) k_histogram(const int32_t* __restrict__ lab, int32_t n, int32_t* vol) {
   const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   const int32_t l = v < n ? lab[v] : -1;
-  const uint32_t m = __match_any_sync(kFull, (uint32_t)l);
-  if (l >= 0 && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(vol + l, __popc(m));
+  const int32_t l0 = __shfl_sync(kFull, l, 0);
+  const uint32_t m0 = __ballot_sync(kFull, l == l0);
+  if (l < 0) return;
+  if (l != l0) atomicAdd(vol + l, 1);
+  else if ((threadIdx.x & 31) == 0) atomicAdd(vol + l, __popc(m0));
 }
 
 // ------------------------------------------------------------------- SLPA

@@ -66,7 +66,7 @@ def test_planner_tiers():
     rc, out = _plan(off, hub_chunk=4096)
     assert rc == 0
     assert out[:7] == [1, 2, 2, 2, 2, 2, 3]  # isolated, tiny, g16, g32, mid, big, hub
-    assert out[7] == 1 + 2 + 3  # hub hash buckets: ceil(deg / 8192)
+    assert out[7] == 2 + 4 + 8  # hub hash buckets: ceil(3 * deg / 8192)
     assert out[15] == 2 + 3 + 5  # hub streaming chunks of 4096 edges
     assert out[9] == 9 and out[14] == 4097 + 10000 + 20000
     rc, out = _plan(off, tiny_max=4, mid_max=64, big_max=512, hub_chunk=256)
