@@ -301,7 +301,7 @@ def run_glp(args, ws, rank, local):
     # end to end through the public API with host buffers
     off_h = g.offsets.cpu().pin_memory()
     cols_h = g.cols.cpu().pin_memory()
-    host_csr = CSR(off_h, cols_h)
+    host_csr = CSR(off_h, cols_h, None, g.symmetric)
     lab_h = None
     for _ in range(1):  # warm the host path once
         h2 = Graph(host_csr)

@@ -176,21 +176,60 @@ static int zeroed(DevicePlan* p, size_t count, T** out) {
   return GLP_OK;
 }
 
+static int ensure_host_offsets(glp_graph* g);
+static int device_bounds(glp_graph* g, const int32_t* thr, int k, int32_t* out);
+
+// Range-mode tier of a degree-sorted graph.
+static Verts range_verts(int32_t lo, int32_t hi) { return Verts{nullptr, lo, hi > lo ? hi - lo : 0}; }
+
 static int ensure_plan(glp_graph* g, const TierParams& t) {
   if (g->plan.valid && g->plan.tiers == t) return GLP_OK;
   free_plan(&g->plan);
   HostPlan hp;
-  build_host_plan(g->h_off.data(), g->n, t, &hp);
   DevicePlan& p = g->plan;
   p.tiers = t;
-  p.isolated = hp.isolated;
   int rc;
-  if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
-      (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
-      (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
-      (rc = upload_verts(&p, hp.big_lo, &p.big_lo)) || (rc = upload_verts(&p, hp.big_hi, &p.big_hi)) ||
-      (rc = zeroed(&p, 9, &p.counts)) || (rc = zeroed(&p, std::max<size_t>(hp.mid.size(), 1), &p.fmid.ids)) ||
-      (rc = zeroed(&p, std::max<size_t>(hp.big.size(), 1), &p.fbig.ids)) || (rc = zeroed(&p, 1, &p.d_mode)) ||
+  int64_t n_mid = 0, n_big = 0, ntier[5] = {0, 0, 0, 0, 0};
+  if (g->deg_sorted == 1) {
+    // every tier is a contiguous range: its bounds come from binary searches
+    // over the non-increasing degrees; only the hubs' offsets reach the host
+    const int32_t thr[7] = {t.big_max, std::min<int32_t>(kBigSplit, t.big_max), t.mid_max, 32, 16, t.tiny_max, 0};
+    int32_t b[7];
+    if ((rc = device_bounds(g, thr, 7, b))) return rc;
+    b[1] = std::min(std::max(b[1], b[0]), b[2]);
+    std::vector<int32_t> hub_off((size_t)b[0] + 1);
+    GLP_CUDA(cudaMemcpy(hub_off.data(), g->d_off, sizeof(int32_t) * hub_off.size(), cudaMemcpyDeviceToHost));
+    build_host_plan(hub_off.data(), b[0], t, &hp);  // all of them are hubs
+    p.big_hi = range_verts(b[0], b[1]);
+    p.big_lo = range_verts(b[1], b[2]);
+    p.big = range_verts(b[0], b[2]);
+    p.mid = range_verts(b[2], b[3]);
+    p.mb = range_verts(b[0], b[3]);
+    p.g32 = range_verts(b[3], b[4]);
+    p.g16 = range_verts(b[4], b[5]);
+    p.tiny = range_verts(b[5], b[6]);
+    p.isolated = g->n - b[6];
+  } else {
+    if ((rc = ensure_host_offsets(g))) return rc;
+    build_host_plan(g->h_off.data(), g->n, t, &hp);
+    p.isolated = hp.isolated;
+    if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
+        (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
+        (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
+        (rc = upload_verts(&p, hp.big_lo, &p.big_lo)) || (rc = upload_verts(&p, hp.big_hi, &p.big_hi))) {
+      free_plan(&p);
+      return rc;
+    }
+  }
+  n_mid = p.mid.n;
+  n_big = p.big.n;
+  ntier[0] = p.tiny.n;
+  ntier[1] = p.g16.n;
+  ntier[2] = p.g32.n;
+  ntier[3] = p.mid.n;
+  ntier[4] = p.big.n;
+  if ((rc = zeroed(&p, 9, &p.counts)) || (rc = zeroed(&p, std::max<size_t>((size_t)n_mid, 1), &p.fmid.ids)) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)n_big, 1), &p.fbig.ids)) || (rc = zeroed(&p, 1, &p.d_mode)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.front.act)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[0])) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[1]))) {
@@ -203,15 +242,12 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   p.front.tiny_max = t.tiny_max;
   p.front.mid_max = t.mid_max;
   p.front.big_max = t.big_max;
-  {
-    const std::vector<int32_t>* lists[5] = {&hp.tiny, &hp.g16, &hp.g32, &hp.mid, &hp.big};
-    for (int k = 0; k < 5; ++k) {
-      if ((rc = zeroed(&p, std::max<size_t>(lists[k]->size(), 1), &p.front.tier[k].ids))) {
-        free_plan(&p);
-        return rc;
-      }
-      p.front.tier[k].count = p.counts + 2 + k;
+  for (int k = 0; k < 5; ++k) {
+    if ((rc = zeroed(&p, std::max<size_t>((size_t)ntier[k], 1), &p.front.tier[k].ids))) {
+      free_plan(&p);
+      return rc;
     }
+    p.front.tier[k].count = p.counts + 2 + k;
   }
   p.n_hubs = (int32_t)hp.hub_v.size();
   p.n_chunks = (int32_t)hp.chunk_hub.size();
@@ -560,7 +596,7 @@ static int ensure_sorted(glp_graph* g) {
   uint32_t* d_bad = nullptr;
   GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
   GLP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), g->stream));
-  k_check_sorted<<<148 * 16, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, d_bad);
+  k_check_sorted<<<148 * 32, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, d_bad);
   uint32_t bad = 1;
   GLP_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, g->stream));
   GLP_CUDA(cudaStreamSynchronize(g->stream));
@@ -743,6 +779,26 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
 }
 
 // ------------------------------------------------------------ validation
+// Offsets: off[0] = 0, off[n] = m, monotone (bad 16 / 8); also the largest
+// degree and whether degrees never increase along the ids (sorted = 0 when
+// some degree is larger than its predecessor's).
+__global__ void k_validate_offsets(const int32_t* __restrict__ off, int32_t n, int64_t m, uint32_t* bad,
+                                   int32_t* maxdeg, uint32_t* unsorted) {
+  for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x) {
+    if (v == 0 && off[0] != 0) atomicOr(bad, 16u);
+    if (v == n) {
+      if ((int64_t)off[n] != m) atomicOr(bad, 16u);
+      continue;
+    }
+    const int32_t d = off[v + 1] - off[v];
+    if (d < 0) atomicOr(bad, 8u);
+    atomicMax(maxdeg, d);
+    if (v + 1 < n && off[v + 2] - off[v + 1] > d) atomicOr(unsorted, 1u);
+  }
+}
+
+// Columns in [0, n) (bad 1), weights >= 0 (bad 2), per-vertex weight sums
+// below 2^31 (bad 4).  Runs only on valid offsets.
 __global__ void k_validate(const int32_t* __restrict__ off, const int32_t* __restrict__ cols,
                            const int32_t* __restrict__ w, int64_t m, int32_t n, uint32_t* bad) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
@@ -760,27 +816,81 @@ __global__ void k_validate(const int32_t* __restrict__ off, const int32_t* __res
 }
 
 int validate_csr_device(glp_graph* g) {
-  if (g->m == 0) return GLP_OK;
-  uint32_t* d_bad = nullptr;
-  GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
-  GLP_CUDA(cudaMemset(d_bad, 0, sizeof(uint32_t)));
-  k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, d_bad);
-  uint32_t bad = 0;
-  cudaError_t e = cudaMemcpy(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost);
-  cudaFree(d_bad);
+  struct Flags {
+    uint32_t bad;
+    int32_t maxdeg;
+    uint32_t unsorted;
+  };
+  Flags* d_f = nullptr;
+  GLP_CUDA(cudaMalloc(&d_f, sizeof(Flags)));
+  GLP_CUDA(cudaMemset(d_f, 0, sizeof(Flags)));
+  k_validate_offsets<<<1184, 256>>>(g->d_off, g->n, g->m, &d_f->bad, &d_f->maxdeg, &d_f->unsorted);
+  Flags f{};
+  cudaError_t e = cudaMemcpy(&f, d_f, sizeof f, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && !f.bad && g->m) {
+    k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, &d_f->bad);
+    e = cudaMemcpy(&f.bad, &d_f->bad, sizeof f.bad, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d_f);
   if (e != cudaSuccess) return cuda_fail(e, "validate");
-  if (bad & 1u) {
+  if (f.bad & 16u) {
+    set_error("offsets[0] must be 0 and offsets[n] must be m");
+    return GLP_EINVAL;
+  }
+  if (f.bad & 8u) {
+    set_error("offsets not monotone");
+    return GLP_EINVAL;
+  }
+  if (f.bad & 1u) {
     set_error("column index outside [0, n)");
     return GLP_EINVAL;
   }
-  if (bad & 2u) {
+  if (f.bad & 2u) {
     set_error("negative edge weight");
     return GLP_EINVAL;
   }
-  if (bad & 4u) {
+  if (f.bad & 4u) {
     set_error("a vertex's weight sum reaches 2^31");
     return GLP_EINVAL;
   }
+  g->max_degree = f.maxdeg;
+  g->deg_sorted = f.unsorted ? 0 : 1;
+  return GLP_OK;
+}
+
+// First vertex whose degree is <= t, for each threshold (degrees must not
+// increase along the ids).
+__global__ void k_tier_bounds(const int32_t* __restrict__ off, int32_t n, const int32_t* thr, int32_t k,
+                              int32_t* out) {
+  const int i = threadIdx.x;
+  if (i >= k) return;
+  const int32_t t = thr[i];
+  int32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int32_t mid = (int32_t)(((int64_t)lo + hi) >> 1);
+    if (off[mid + 1] - off[mid] <= t) hi = mid; else lo = mid + 1;
+  }
+  out[i] = lo;
+}
+
+// Host copy of the offsets, made on first need (unsorted graphs, reports).
+static int ensure_host_offsets(glp_graph* g) {
+  if (!g->h_off.empty()) return GLP_OK;
+  g->h_off.resize((size_t)g->n + 1);
+  GLP_CUDA(cudaMemcpy(g->h_off.data(), g->d_off, sizeof(int32_t) * ((size_t)g->n + 1), cudaMemcpyDeviceToHost));
+  return GLP_OK;
+}
+
+static int device_bounds(glp_graph* g, const int32_t* thr, int k, int32_t* out) {
+  int32_t* d = nullptr;
+  GLP_CUDA(cudaMalloc(&d, sizeof(int32_t) * 2 * k));
+  cudaError_t e = cudaMemcpy(d, thr, sizeof(int32_t) * k, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_tier_bounds<<<1, 32>>>(g->d_off, g->n, d, k, d + k);
+    e = cudaMemcpy(out, d + k, sizeof(int32_t) * k, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "tier bounds");
   return GLP_OK;
 }
 
@@ -897,27 +1007,7 @@ int glp_graph_create_ex(const int32_t* offsets, const int32_t* cols, const int32
   g->n = n;
   g->m = m;
   GLP_CUDA(cudaGetDevice(&g->device));
-  g->h_off.resize((size_t)n + 1);
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  if (on_device)
-    GLP_CUDA(cudaMemcpy(g->h_off.data(), offsets, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost));
-  else
-    std::memcpy(g->h_off.data(), offsets, sizeof(int32_t) * ((size_t)n + 1));
-  // validate offsets on the host (they are needed there for planning anyway)
-  if (g->h_off[0] != 0 || (int64_t)g->h_off[n] != m) {
-    set_error("offsets[0]=%d, offsets[n]=%d, m=%lld", g->h_off[0], g->h_off[n], (long long)m);
-    return GLP_EINVAL;
-  }
-  int32_t maxd = 0;
-  for (int32_t v = 0; v < n; ++v) {
-    const int32_t d = g->h_off[v + 1] - g->h_off[v];
-    if (d < 0) {
-      set_error("offsets not monotone at vertex %d", v);
-      return GLP_EINVAL;
-    }
-    maxd = std::max(maxd, d);
-  }
-  g->max_degree = maxd;
   GLP_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
   GLP_CUDA(cudaStreamCreateWithFlags(&g->aux[0], cudaStreamNonBlocking));
   GLP_CUDA(cudaStreamCreateWithFlags(&g->aux[1], cudaStreamNonBlocking));
@@ -925,7 +1015,7 @@ int glp_graph_create_ex(const int32_t* offsets, const int32_t* cols, const int32
   GLP_CUDA(cudaEventCreateWithFlags(&g->join[0], cudaEventDisableTiming));
   GLP_CUDA(cudaEventCreateWithFlags(&g->join[1], cudaEventDisableTiming));
   GLP_CUDA(cudaMalloc(&g->d_off, sizeof(int32_t) * ((size_t)n + 1)));
-  GLP_CUDA(cudaMemcpy(g->d_off, g->h_off.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice));
+  GLP_CUDA(cudaMemcpy(g->d_off, offsets, sizeof(int32_t) * ((size_t)n + 1), kind));
   // 4 padding entries: tile kernels read columns as aligned 16-byte quads
   GLP_CUDA(cudaMalloc(&g->d_cols, sizeof(int32_t) * (m + 4)));
   GLP_CUDA(cudaMemset(g->d_cols + m, 0, sizeof(int32_t) * 4));
@@ -1011,6 +1101,8 @@ int glp_graph_plan(glp_graph* g, const glp_params* p, int64_t out[16]) {
     set_error("graph is NULL");
     return GLP_EINVAL;
   }
+  int rc = ensure_host_offsets(g);
+  if (rc) return rc;
   return glp_plan_offsets(g->h_off.data(), g->n, p, out);
 }
 

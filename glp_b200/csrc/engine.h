@@ -101,7 +101,7 @@ struct glp_graph {
   int32_t* d_off = nullptr;
   int32_t* d_cols = nullptr;
   int32_t* d_w = nullptr;
-  std::vector<int32_t> h_off;
+  std::vector<int32_t> h_off;  // host copy of the offsets, made on first need
   cudaStream_t stream = nullptr;
   glp::DevicePlan plan;
   // work buffers (grown on demand)
@@ -118,6 +118,7 @@ struct glp_graph {
   double* d_hook_vals = nullptr;
   int symmetric = -1;    // -1 unknown, 0 no, 1 yes (every edge stored both ways)
   int rows_sorted = -1;  // -1 unknown, 0 no, 1 every row strictly ascending
+  int deg_sorted = 0;    // 1: degrees never increase along the vertex ids
   uint32_t epoch = 0;  // frontier mark of the last step
   // auxiliary streams and fork/join events of a step
   cudaStream_t aux[2] = {nullptr, nullptr};

@@ -749,16 +749,23 @@ __global__ void __launch_bounds__(256) k_first_step(StepArgs a) {
   }
 }
 
-// bad |= 1 when some row is not strictly ascending.
-__global__ void k_check_sorted(const int32_t* __restrict__ off, const int32_t* __restrict__ cols, int32_t n,
-                               uint32_t* bad) {
-  for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+// bad |= 1 when some row is not strictly ascending.  One warp per row, 8
+// column pairs in flight per lane.
+__global__ void __launch_bounds__(256) k_check_sorted(const int32_t* __restrict__ off,
+                                                      const int32_t* __restrict__ cols, int32_t n, uint32_t* bad) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
     const int32_t b = off[v], e = off[v + 1];
-    for (int32_t j = b + 1; j < e; ++j)
-      if (cols[j - 1] >= cols[j]) {
-        atomicOr(bad, 1u);
-        break;
+    bool ok = true;
+    for (int32_t j0 = b + 1 + lane; j0 < e; j0 += 256) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int32_t j = j0 + 32 * q;
+        if (j < e && ld_stream(cols + j - 1) >= ld_stream(cols + j)) ok = false;
       }
+    }
+    if (__any_sync(kFull, !ok) && lane == 0) atomicOr(bad, 1u);
   }
 }
 
