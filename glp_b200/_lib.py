@@ -108,6 +108,8 @@ SIGNATURES = {
     "glp_load_edgelist_bin": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "glp_free_host": (None, [C.c_void_p]),
+    "glp_run_classic_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p,
+                                          C.c_void_p, C.c_void_p]),
 }
 
 OPTIONAL_SIGNATURES: dict = {}

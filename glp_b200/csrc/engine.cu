@@ -10,6 +10,8 @@
 //   run_layered           <- MultiLprop::perform_lp loop (prop/MultiLprop.cuh:308-374)
 //   run_slpa              <- SLPA loop (tutorial/Base5prop.cuh:264-293)
 #include <algorithm>
+#include <atomic>
+#include <cstddef>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
@@ -954,6 +956,85 @@ static int run_hooks(RunCtx& c, const glp_params& p, int32_t niter) {
   return hooks_iterations(c, HooksWeightedDegree{st}, niter, 0, false, &vr, &vw);
 }
 
+
+// ------------------------------------------------- allocation-free classic LP
+// Scratch of glp_run_classic_noalloc: one copy per device (module globals are
+// per context), found with cudaGetSymbolAddress.
+constexpr int32_t kNoAllocMaxVertices = 1 << 20;
+constexpr int32_t kNoAllocMaxIters = 4096;
+constexpr int32_t kNoAllocMaxDegree = 4096;
+constexpr int kNoAllocNT = 128;
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocScratch {
+  int32_t labels[kNoAllocMaxVertices];           // the second label buffer
+  unsigned long long changed[kNoAllocMaxIters];  // per-iteration change counts
+  uint32_t err;                                  // kErr* bits of the steps
+  uint32_t bad;                                  // validation bits
+  int32_t maxdeg;
+  uint32_t unsorted;
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+static std::atomic<void*> g_noalloc_ptr[kNoAllocMaxDevices];
+
+static inline size_t pow2_host(int32_t x) {
+  size_t p = 1;
+  while (p < (size_t)x) p <<= 1;
+  return p;
+}
+
+// One classic step over every vertex, a block per vertex: the k_big counting
+// (shared table of pow2(2*degree) slots, running maxima) extended to degree 0,
+// where the vertex keeps its label.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_noalloc_step(const int32_t* __restrict__ off,
+                                                      const int32_t* __restrict__ cols,
+                                                      const int32_t* __restrict__ lin, int32_t* __restrict__ lout,
+                                                      int32_t n, unsigned long long* changed, uint32_t* err) {
+  extern __shared__ __align__(8) uint32_t smem[];
+  __shared__ Best red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const ScoreClassic score;
+  for (int32_t v = blockIdx.x; v < n; v += gridDim.x) {
+    const int32_t b = off[v], e = off[v + 1];
+    if (b == e) {  // block-uniform
+      if (threadIdx.x == 0) lout[v] = lin[v];
+      continue;
+    }
+    const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));
+    uint32_t* keys = smem;
+    uint32_t* vals = smem + cap;
+    for (uint32_t s = threadIdx.x; s < 2 * cap; s += NT) smem[s] = 0;
+    __syncthreads();
+    Best best = best_none();
+    bool fail = false;
+    auto ins = [&](uint32_t key, uint32_t k) {
+      return table_insert_bounded(keys, vals, cap - 1, key, k, cap, nullptr, nullptr);
+    };
+    for (int32_t j0 = b + warp * 32; j0 < e; j0 += 4 * NT) {
+      int32_t lab[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int32_t j = j0 + q * NT + lane;
+        lab[q] = j < e ? ld_stream(cols + j) : -1;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (lab[q] >= 0) lab[q] = ld_label(lin + lab[q]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (j0 + q * NT < e) count_chunk<false>(lab[q] >= 0, lab[q], 1u, score, ins, best, fail);
+    }
+    if (fail) atomicOr(err, kErrProbe);
+    best = block_max<NT>(best, red);
+    if (threadIdx.x == 0) {
+      lout[v] = best.l;
+      if (best.l != lin[v]) atomicAdd(changed, 1ull);
+    }
+  }
+}
+
 }  // namespace glp
 
 using namespace glp;
@@ -1247,5 +1328,98 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
 }
 
 void glp_free_host(void* p) { std::free(p); }
+
+int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int32_t n, int64_t m, int32_t niter,
+                            int32_t* d_labels, int64_t* changed, void* stream) {
+  if (n < 0 || m < 0 || niter < 0 || !d_offsets || !d_labels || (m > 0 && !d_cols)) {
+    set_error("bad arguments (n=%d, m=%lld, niter=%d)", n, (long long)m, niter);
+    return GLP_EINVAL;
+  }
+  if (n > kNoAllocMaxVertices) {
+    set_error("n=%d exceeds the allocation-free limit of %d vertices", n, kNoAllocMaxVertices);
+    return GLP_EINVAL;
+  }
+  if (niter > kNoAllocMaxIters) {
+    set_error("niter=%d exceeds the allocation-free limit of %d iterations", niter, kNoAllocMaxIters);
+    return GLP_EINVAL;
+  }
+  if (m > INT32_MAX) {
+    set_error("m=%lld exceeds int32 CSR", (long long)m);
+    return GLP_EINVAL;
+  }
+  int rc = require_device();
+  if (rc) return rc;
+  int dev = 0;
+  GLP_CUDA(cudaGetDevice(&dev));
+  if (dev >= kNoAllocMaxDevices) {
+    set_error("device %d beyond the %d devices the allocation-free path tracks", dev, kNoAllocMaxDevices);
+    return GLP_ENOTSUP;
+  }
+  // set-up, once per device, with that device current
+  void* sp = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (!sp) {
+    const cudaError_t e = cudaGetSymbolAddress(&sp, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(allocation-free scratch)");
+    GLP_CUDA(cudaFuncSetAttribute(k_noalloc_step<kNoAllocNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * pow2_host(2 * kNoAllocMaxDegree) * sizeof(uint32_t))));
+    g_noalloc_ptr[dev].store(sp, std::memory_order_release);
+  }
+  NoAllocScratch* sc = static_cast<NoAllocScratch*>(sp);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // counters and flags start at zero; the label buffers are written below
+  GLP_CUDA(cudaMemsetAsync(sc->changed, 0, sizeof(NoAllocScratch) - offsetof(NoAllocScratch, changed), st));
+  if (n == 0) {
+    if (m != 0) {
+      set_error("offsets[0] must be 0 and offsets[n] must be m");
+      return GLP_EINVAL;
+    }
+    GLP_CUDA(cudaStreamSynchronize(st));
+    for (int32_t i = 0; changed && i < niter; ++i) changed[i] = 0;
+    return GLP_OK;
+  }
+  k_validate_offsets<<<1184, 256, 0, st>>>(d_offsets, n, m, &sc->bad, &sc->maxdeg, &sc->unsorted);
+  if (m) k_validate<<<1184, 256, 0, st>>>(d_offsets, d_cols, nullptr, m, n, &sc->bad);
+  GLP_CUDA(cudaGetLastError());
+  uint32_t flags[2] = {0, 0};  // bad, maxdeg
+  GLP_CUDA(cudaMemcpyAsync(flags, &sc->bad, sizeof flags, cudaMemcpyDeviceToHost, st));
+  GLP_CUDA(cudaStreamSynchronize(st));
+  if (flags[0] & 16u) {
+    set_error("offsets[0] must be 0 and offsets[n] must be m");
+    return GLP_EINVAL;
+  }
+  if (flags[0] & 8u) {
+    set_error("offsets not monotone");
+    return GLP_EINVAL;
+  }
+  if (flags[0] & 1u) {
+    set_error("column index outside [0, n)");
+    return GLP_EINVAL;
+  }
+  const int32_t maxdeg = (int32_t)flags[1];
+  if (maxdeg > kNoAllocMaxDegree) {
+    set_error("a vertex of degree %d exceeds the allocation-free limit of %d", maxdeg, kNoAllocMaxDegree);
+    return GLP_EINVAL;
+  }
+  int32_t* buf[2] = {d_labels, sc->labels};
+  k_iota<<<(unsigned)cdiv(n, 256), 256, 0, st>>>(buf[0], buf[1], n);
+  const size_t smem = 2 * pow2_host(2 * std::max(maxdeg, 1)) * sizeof(uint32_t);
+  const unsigned grid = (unsigned)std::min<int64_t>(n, 148 * 16);
+  for (int32_t it = 0; it < niter; ++it)
+    k_noalloc_step<kNoAllocNT><<<grid, kNoAllocNT, smem, st>>>(d_offsets, d_cols, buf[it & 1], buf[(it + 1) & 1], n,
+                                                               sc->changed + it, &sc->err);
+  GLP_CUDA(cudaGetLastError());
+  if (niter & 1) GLP_CUDA(cudaMemcpyAsync(d_labels, sc->labels, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+  uint32_t err = 0;
+  GLP_CUDA(cudaMemcpyAsync(&err, &sc->err, sizeof err, cudaMemcpyDeviceToHost, st));
+  static_assert(sizeof(int64_t) == sizeof(unsigned long long), "changed counts are 64-bit");
+  if (changed && niter)
+    GLP_CUDA(cudaMemcpyAsync(changed, sc->changed, sizeof(int64_t) * niter, cudaMemcpyDeviceToHost, st));
+  GLP_CUDA(cudaStreamSynchronize(st));
+  if (err) {
+    set_error("kernel error flags 0x%x", err);
+    return GLP_EKERNEL;
+  }
+  return GLP_OK;
+}
 
 }  // extern "C"

@@ -188,6 +188,26 @@ int glp_load_edgelist_bin(const char* path, int32_t direct, int32_t** offsets, i
                           int64_t* m);
 void glp_free_host(void* p);
 
+/* ----------------------------------------------------------------------
+ * Allocation-free classic LP.  No counterpart in the reference.
+ *
+ * Method 1 (classic, unweighted; the rule of glp_run) for niter iterations
+ * over a CSR the caller already holds on the current device, with labels
+ * starting at the vertex ids and written to d_labels (device, n entries).
+ * The call allocates no device or pinned host memory: its second label
+ * buffer, per-iteration change counters and flag words live in a fixed
+ * static device array (about 4.2 MB per device).  Limits: n <= 1048576
+ * vertices, niter <= 4096, every degree <= 4096; larger inputs, like a
+ * malformed CSR, return GLP_EINVAL with the limit in glp_last_error().
+ * `changed` (host, nullable) receives niter change counts.  Work runs on
+ * `stream` (NULL: the legacy default stream) and the call returns after it
+ * has finished.  The first call on each device looks up that device's scratch
+ * (cudaGetSymbolAddress); make it before any stream capture.  The scratch is
+ * shared: calls on one device that overlap (from several host threads) race
+ * and must be serialised by the caller. */
+int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int32_t n, int64_t m, int32_t niter,
+                            int32_t* d_labels, int64_t* changed, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
