@@ -60,6 +60,14 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=1)
+    ap.add_argument("--workload", default="classic", choices=["classic", "batched"],
+                    help="classic: the R-MAT headline line (with a batched summary unless --no-batched); "
+                         "batched: the batched workload alone")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--graphs", type=int, default=4096, help="batched workload: number of graphs")
+    ap.add_argument("--batch-seed", type=int, default=5)
+    ap.add_argument("--plain-sample", type=int, default=256,
+                    help="batched workload: graphs timed through the one-graph-at-a-time engine")
     return ap.parse_args()
 
 
@@ -378,8 +386,155 @@ def run_glp(args, ws, rank, local):
             "clocks": clk,
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line))
     handle.close()
+    del handle, labels_dev, g
+    torch.cuda.empty_cache()
+    if not args.no_batched:
+        bl = run_batched(args, ws, rank, local)
+        if rank == 0:
+            line["batched"] = {k: bl[k] for k in ("metric", "value", "unit", "ms_per_step", "config", "plain",
+                                                 "vs_plain", "e2e", "roofline", "cpu_baseline")}
+    if rank == 0:
+        print(json.dumps(line))
+
+
+# ----------------------------------------------------------------- batched
+def run_batched(args, ws, rank, local, embed=False):
+    """The batched workload: `args.graphs` planted-partition graphs (vertex
+    counts log-uniform in [1k, 200k], 4-64 communities, mean degree
+    log-uniform in [4, 64], seed --batch-seed), 20 classic iterations each,
+    all of them in one persistent launch per step (CUDA-graph replay, labels
+    left on the device).  Against the one-graph-at-a-time engine on a
+    systematic sample of the same graphs (handles resident, labels on the
+    device), and, end to end, against packing from host buffers + a run with
+    labels back to the host."""
+    from glp_b200 import _lib, graphs
+    from glp_b200.batch import Batch
+    from glp_b200.engine import Graph, make_params
+
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    t0 = time.time()
+    gs = graphs.batch_planted(args.graphs, args.batch_seed, device=dev)
+    torch.cuda.synchronize(dev)
+    gen_s = time.time() - t0
+    n = sum(g.n for g in gs)
+    m = sum(g.m for g in gs)
+    b = Batch(gs)
+    t0 = time.time()
+    best, cand_ms = b.tune(3)
+    tune_s = time.time() - t0
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    out = torch.empty(max(b.n, 1), dtype=torch.int32, device=dev)
+    pg = make_params(use_graph=1)
+    for _ in range(args.warmup):
+        b.run(args.iters, pg, labels_out=out, stream=sp, changed=False)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        b.run(args.iters, pg, labels_out=out, stream=sp, changed=False)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    ms = max_over_ranks(ws, ev0.elapsed_time(ev1))
+    total_graphs = sum_over_ranks(ws, float(args.graphs * args.steps))
+    value = total_graphs / (ms / 1e3)
+    labels = out[:b.n].cpu().numpy()
+
+    # plain engine: a systematic sample, handles resident, labels on the device
+    idx = list(range(0, args.graphs, max(1, args.graphs // max(1, args.plain_sample))))
+    hs = [Graph(gs[i]) for i in idx]
+    outs = [torch.empty(max(h.n, 1), dtype=torch.int32, device=dev) for h in hs]
+    for h, o in zip(hs[:4], outs[:4]):
+        h.run(_lib.METHOD_CLASSIC, args.iters, labels_out=o, stream=sp)
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    for h, o in zip(hs, outs):
+        h.run(_lib.METHOD_CLASSIC, args.iters, labels_out=o, stream=sp)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = ev0.elapsed_time(ev1)
+    mismatch = sum(int(not np.array_equal(o[:h.n].cpu().numpy(), labels[b.vbase[i]:b.vbase[i + 1]]))
+                   for i, h, o in zip(idx, hs, outs))
+    for h in hs:
+        h.close()
+    del hs, outs
+    plain_value = len(idx) / (plain_ms / 1e3)
+
+    # end to end: host buffers in, packing + run + labels out, every step
+    host = [graphs.CSR(g.offsets.cpu().pin_memory(), g.cols.cpu().pin_memory(), None, g.symmetric) for g in gs]
+    h2d = int(sum(4 * (g.n + 1 + g.m) for g in gs))
+    e2e_steps = max(1, min(args.e2e_steps, 2))
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    same = True
+    for _ in range(e2e_steps):
+        with Batch(host) as bh:
+            lab_h, _ = bh.run(args.iters, changed=False)
+        same = same and bool(np.array_equal(lab_h, labels))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    e2e_value = sum_over_ranks(ws, float(args.graphs * e2e_steps)) / (e2e_ms / 1e3)
+    del host
+
+    # roofline: 8 B per CSR entry (column + gathered label), 8 B offset +
+    # 4 B own label + 4 B written label per vertex, per iteration
+    bytes_iter = 8 * m + 16 * n + 8
+    iter_ms = ms / (args.steps * args.iters)
+    peak, peak_kind = measured_peak()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            k = 4
+            times = []
+            with tempfile.TemporaryDirectory() as d:
+                for g in gs[:k]:
+                    path = os.path.join(d, "g.csr")
+                    write_csr(path, g.offsets.cpu().numpy(), g.cols.cpu().numpy())
+                    times.append(sum(ref_cpulp_run(path, args.iters)))
+            cpu = {"value": round(k / sum(times), 3), "unit": "graphs/s", "cores": cpu_threads_used(),
+                   "kind": "reference",
+                   "sample": f"reference CPUlp::sync_run_1 (tutorial/CPUlp.cuh, built from source), first {k} graphs "
+                             f"of the batch x {args.iters} iterations, {sum(times):.2f} s"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "graphs/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    res = {
+        "metric": f"batched classic LP graphs/s ({args.graphs} planted-partition graphs, {args.iters} iterations)",
+        "value": round(value, 1), "unit": "graphs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic planted-partition batch (seeded), generated on the GPU",
+        "config": {"workload": f"batch{args.graphs}-planted-seed{args.batch_seed}-classic-{args.iters}it",
+                   "graphs": args.graphs, "n": n, "m": m, "parallelism": f"replicas{ws}",
+                   "l2": "inputs larger than L2 (CSR %.1f GB); no flush" % (4 * (n + 1 + m) / 1e9),
+                   "launch": "one persistent cooperative launch per step, CUDA-graph replay",
+                   "tuned": {"threads": best.reserved[0], "thread_tier_max": best.tiny_max,
+                             "warp_tier_max": best.mid_max},
+                   "tune_s": round(tune_s, 2), "graph_gen_s": round(gen_s, 2)},
+        "plain": {"value": round(plain_value, 1), "unit": "graphs/s", "sample_graphs": len(idx),
+                  "sample_vertex_frac": round(sum(gs[i].n for i in idx) / n, 4),
+                  "labels_match_batch": mismatch == 0,
+                  "how": "glp_run method 1 per graph, handles resident, labels on the device"},
+        "vs_plain": round(value / plain_value, 2),
+        "e2e": {"value": round(e2e_value, 1), "unit": "graphs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(4 * n), "steps": e2e_steps, "labels_match_device_run": same},
+        "gpu_launches": int(args.steps),
+        "roofline": {"bound": "hbm", "achieved": round(bytes_iter / (iter_ms / 1e3) / 1e9, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(bytes_iter / (iter_ms / 1e3) / 1e9 / peak, 4), "traffic": None,
+                     "kernel": "k_batch", "peak_kind": peak_kind, "bytes_per_iter": int(bytes_iter),
+                     "iter_ms": round(iter_ms, 4)},
+        "cpu_baseline": cpu,
+    }
+    b.close()
+    del gs
+    torch.cuda.empty_cache()
+    return res
 
 
 def main():
@@ -387,6 +542,10 @@ def main():
     ws, rank, local = dist_init(args)
     if args.impl == "reference":
         run_reference(args, ws, rank)
+    elif args.workload == "batched":
+        res = run_batched(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(res))
     else:
         run_glp(args, ws, rank, local)
     if ws > 1:

@@ -108,6 +108,13 @@ SIGNATURES = {
     "glp_load_edgelist_bin": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "glp_free_host": (None, [C.c_void_p]),
+    "glp_batch_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                   C.POINTER(C.c_void_p)]),
+    "glp_batch_destroy": (None, [C.c_void_p]),
+    "glp_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_int32)]),
+    "glp_batch_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "glp_batch_tune": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "glp_run_classic_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p,
                                           C.c_void_p, C.c_void_p]),
 }

@@ -173,3 +173,38 @@ def from_edges(n: int, edges, relabel: bool = False) -> CSR:
     """Small hand-made graphs: an undirected edge list -> symmetric CSR."""
     e = np.asarray(edges, dtype=np.int32).reshape(-1, 2)
     return build_csr(torch.from_numpy(e[:, 0].copy()), torch.from_numpy(e[:, 1].copy()), n, relabel=relabel)
+
+
+# ------------------------------------------------------------ batched workload
+_M64 = (1 << 64) - 1
+
+
+def _splitmix64(x: int) -> int:
+    x = (x + 0x9E3779B97F4A7C15) & _M64
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def batch_specs(count: int, seed: int, n_range=(1000, 200000), k_range=(4, 64), deg_range=(4.0, 64.0),
+                intra_frac: float = 0.85) -> list[dict]:
+    """Per-graph parameters of the batched workload: vertex count log-uniform
+    in n_range, communities uniform in k_range, mean degree log-uniform in
+    deg_range (intra_frac of it inside the community).  Counter based:
+    graph i depends only on (seed, i)."""
+    out = []
+    for i in range(count):
+        u = [_splitmix64(_splitmix64(seed) ^ (i * 4 + j)) / 2.0 ** 64 for j in range(4)]
+        n = int(round(math.exp(math.log(n_range[0]) + u[0] * (math.log(n_range[1]) - math.log(n_range[0])))))
+        k = k_range[0] + min(int(u[1] * (k_range[1] - k_range[0] + 1)), k_range[1] - k_range[0])
+        d = math.exp(math.log(deg_range[0]) + u[2] * (math.log(deg_range[1]) - math.log(deg_range[0])))
+        out.append({"n": n, "k": k, "mean_deg": d, "intra": d * intra_frac, "inter": d * (1 - intra_frac),
+                    "seed": _splitmix64(seed * 0x100000001B3 + i) & 0x7FFFFFFFFFFFFFFF})
+    return out
+
+
+def batch_planted(count: int, seed: int, device="cpu", **kw) -> list[CSR]:
+    """The batched workload: `count` planted-partition graphs (batch_specs)."""
+    return [planted(s["n"], s["k"], s["intra"], s["inter"], s["seed"], device=device)
+            for s in batch_specs(count, seed, **kw)]

@@ -189,6 +189,44 @@ int glp_load_edgelist_bin(const char* path, int32_t direct, int32_t** offsets, i
 void glp_free_host(void* p);
 
 /* ----------------------------------------------------------------------
+ * Batched classic LP.  The reference runs one graph per propagator (its
+ * two-graph precursor, tutorial/MultiGprop.cuh:585-800, launches each graph
+ * separately); a batch packs many independent graphs into one
+ * device-resident multi-CSR and propagates all of them in ONE persistent
+ * cooperative kernel launch per run.
+ *
+ * glp_batch_create: graph g is offsets[g] (n[g]+1 int32) and cols[g] (m[g]
+ * int32, ids local to the graph), host or device arrays (on_device),
+ * unweighted.  The packed labels of a run hold graph g's labels at
+ * [vbase_g, vbase_g + n[g]), vbase_g = n[0] + ... + n[g-1]; they equal what
+ * glp_run(method 1) gives that graph alone, bit for bit.  Every degree must
+ * be <= 4096 (GLP_ENOTSUP otherwise: run such a graph with glp_run). */
+typedef struct glp_batch glp_batch;
+int glp_batch_create(int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols, const int32_t* n,
+                     const int64_t* m, int32_t on_device, glp_batch** out);
+void glp_batch_destroy(glp_batch* b);
+int glp_batch_info(const glp_batch* b, int64_t* n, int64_t* m, int32_t* max_degree, int32_t* ngraphs);
+/* niter synchronous classic iterations of every graph.  labels: the packed
+ * labels (host, or device when on_device); changed: optional host [niter]
+ * labels changed per iteration over the batch.  params (nullable; other
+ * values = the tuned or default choice): tiny_max in {8,16,32} = largest
+ * degree counted by one thread per vertex (above it, up to 32, lane groups);
+ * mid_max 64 = degrees 33..64 by 16-lane groups, 32 = by whole warps;
+ * reserved[0] in {512,1024} = threads per block; use_graph = 1 captures the
+ * run (counter resets, the persistent launch, a device-side label copy) in a
+ * CUDA graph once and replays it while niter, the configuration, the stream
+ * and the device label pointer stay the same.  Synchronous with respect to
+ * the host. */
+int glp_batch_run(glp_batch* b, const glp_params* p, int32_t niter, int32_t* labels, int32_t on_device,
+                  int64_t* changed, void* stream);
+/* Autotuner: times every kernel configuration (threads per block x thread
+ * tier bound x counting of degrees 33..64) on this batch for probe_iters iterations and
+ * keeps the fastest for later runs.  best (nullable) receives the choice in
+ * the glp_batch_run parameter fields; times_ms (nullable, >= 12 entries)
+ * the time of each candidate (-1: does not fit); ncand the candidate count. */
+int glp_batch_tune(glp_batch* b, int32_t probe_iters, glp_params* best, float* times_ms, int32_t* ncand);
+
+/* ----------------------------------------------------------------------
  * Allocation-free classic LP.  No counterpart in the reference.
  *
  * Method 1 (classic, unweighted; the rule of glp_run) for niter iterations

@@ -1,0 +1,142 @@
+"""Batched classic LP (glp_batch_*) against one-graph-at-a-time runs.
+
+Every graph's labels out of the packed batch must equal its solo
+``glp_run`` (method 1) labels, and the oracle's, after the same number of
+iterations; per-iteration changed totals must equal the sum over the solo
+runs.  Graphs cover every tier of the batch kernel (thread, warp, block),
+isolated vertices, single-vertex and edgeless graphs, and rows that are not
+strictly ascending (which turns the first-step closed form off).
+"""
+import numpy as np
+import pytest
+import torch
+
+from glp_b200 import _lib, graphs
+from glp_b200.batch import Batch
+from glp_b200.engine import Graph, make_params
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _solo(g, niter):
+    with Graph(g.to("cpu")) as h:
+        r = h.run(_lib.METHOD_CLASSIC, niter)
+    return r.labels, r.changed
+
+
+def _mixed(device="cuda"):
+    gs = [
+        graphs.planted(3000, 8, 10.0, 2.0, seed=11, device=device),
+        graphs.rmat(11, 16, seed=4, device=device),           # degrees into the block tier
+        graphs.planted(1500, 4, 40.0, 6.0, seed=12, device=device),
+        graphs.from_edges(6, [(0, 1), (1, 2), (2, 0), (4, 5)]).to(device),  # vertex 3 isolated
+        graphs.from_edges(1, []).to(device),                  # one isolated vertex
+        graphs.from_edges(300, [(0, 1 + i) for i in range(299)] + [(1, 2), (5, 6)]).to(device),
+        graphs.rmat(9, 8, seed=9, device=device),
+    ]
+    return gs
+
+
+def _check(b, gs, niter, labels, changed):
+    ch_sum = np.zeros(niter, dtype=np.int64)
+    for i, (g, lab) in enumerate(zip(gs, b.split(labels))):
+        ref, ch = _solo(g, niter)
+        np.testing.assert_array_equal(np.asarray(lab), ref, err_msg=f"graph {i}")
+        ch_sum += ch
+    np.testing.assert_array_equal(changed, ch_sum)
+
+
+@pytest.mark.parametrize("niter", [1, 2, 7, 20])
+def test_batch_matches_solo_runs(niter):
+    gs = _mixed()
+    with Batch(gs) as b:
+        labels, changed = b.run(niter)
+        _check(b, gs, niter, labels, changed)
+
+
+def test_batch_matches_oracle():
+    gs = _mixed("cpu")
+    with Batch(gs) as b:
+        labels, _ = b.run(9)
+        for g, lab in zip(gs, b.split(labels)):
+            off, cols, _ = g.numpy()
+            np.testing.assert_array_equal(lab, O.classic_run(off, cols, 9))
+
+
+def test_batch_rows_not_ascending():
+    # reversed rows: same graph, the first step must be counted
+    gs = []
+    for g in _mixed("cpu")[:4]:
+        off, cols, _ = g.numpy()
+        rc = cols.copy()
+        for v in range(len(off) - 1):
+            rc[off[v]:off[v + 1]] = cols[off[v]:off[v + 1]][::-1]
+        gs.append(graphs.from_numpy(off, rc))
+    with Batch(gs) as b:
+        labels, changed = b.run(6)
+        _check(b, gs, 6, labels, changed)
+
+
+def test_batch_every_configuration_agrees():
+    gs = _mixed()
+    with Batch(gs) as b:
+        ref, ref_ch = b.run(8)
+        for nt in (512, 1024):
+            for tt in (8, 16, 32):
+                for mid in (32, 64):
+                    p = make_params(tiny_max=tt, mid_max=mid)
+                    p.reserved[0] = nt
+                    lab, ch = b.run(8, p)
+                    np.testing.assert_array_equal(lab, ref, err_msg=f"{nt} {tt} {mid}")
+                    np.testing.assert_array_equal(ch, ref_ch)
+
+
+def test_batch_tune_graph_replay_and_device_labels():
+    gs = _mixed()
+    with Batch(gs) as b:
+        ref, ref_ch = b.run(12)
+        best, times = b.tune(2)
+        assert len(times) == 12 and (times > 0).any()
+        assert best.tiny_max in (8, 16, 32) and best.mid_max in (32, 64) and best.reserved[0] in (512, 1024)
+        lab, ch = b.run(12)
+        np.testing.assert_array_equal(lab, ref)
+        p = make_params(use_graph=1)
+        out = torch.empty(b.n, dtype=torch.int32, device="cuda")
+        for _ in range(3):  # capture once, replay
+            out.fill_(-1)
+            _, ch = b.run(12, p, labels_out=out)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(out.cpu().numpy(), ref)
+            np.testing.assert_array_equal(ch, ref_ch)
+        lab, _ = b.run(12, p)  # host labels from a replay
+        np.testing.assert_array_equal(lab, ref)
+
+
+def test_batch_host_and_device_inputs_agree():
+    gd = _mixed("cuda")
+    gh = [g.to("cpu") for g in gd]
+    with Batch(gd) as bd, Batch(gh) as bh:
+        np.testing.assert_array_equal(bd.run(5)[0], bh.run(5)[0])
+        assert bd.info()["m"] == sum(g.m for g in gd)
+
+
+def test_batch_rejects_degree_above_limit():
+    star = graphs.from_edges(4098, [(0, 1 + i) for i in range(4097)])
+    with pytest.raises(_lib.GlpError) as e:
+        Batch([graphs.from_edges(4, [(0, 1)]), star])
+    assert e.value.code == _lib.GLP_ENOTSUP
+
+
+def test_batch_rejects_column_outside_its_graph():
+    bad = graphs.from_numpy(np.array([0, 1, 2], np.int32), np.array([1, 2], np.int32))  # column 2 >= n
+    with pytest.raises(_lib.GlpError) as e:
+        Batch([graphs.from_edges(3, [(0, 1)]), bad])
+    assert e.value.code == _lib.GLP_EINVAL
+
+
+def test_batch_workload_sample():
+    gs = graphs.batch_planted(24, 5, device="cuda")
+    with Batch(gs) as b:
+        labels, changed = b.run(20)
+        _check(b, gs, 20, labels, changed)

@@ -66,3 +66,12 @@ def test_weights_symmetric_and_ranged():
     d = {(int(a), int(b)): int(x) for a, b, x in zip(src, cols, w)}
     for (a, b), x in list(d.items())[:2000]:
         assert d[(b, a)] == x
+
+
+def test_batch_specs_are_counter_based():
+    a = graphs.batch_specs(50, 5)
+    b = graphs.batch_specs(80, 5)
+    assert a == b[:50]
+    assert graphs.batch_specs(50, 6) != a
+    for s in b:
+        assert 1000 <= s["n"] <= 200000 and 4 <= s["k"] <= 64 and 4.0 <= s["mean_deg"] <= 64.0
