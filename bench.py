@@ -60,10 +60,14 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=1)
-    ap.add_argument("--workload", default="classic", choices=["classic", "batched"],
+    ap.add_argument("--workload", default="classic", choices=["classic", "batched", "served"],
                     help="classic: the R-MAT headline line (with a batched summary unless --no-batched); "
                          "batched: the batched workload alone")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--requests", type=int, default=300, help="served workload: requests per arrival rate")
+    ap.add_argument("--rates", default="50,200", help="served workload: Poisson arrival rates (req/s)")
+    ap.add_argument("--serve-seed", type=int, default=6)
     ap.add_argument("--graphs", type=int, default=4096, help="batched workload: number of graphs")
     ap.add_argument("--batch-seed", type=int, default=5)
     ap.add_argument("--plain-sample", type=int, default=256,
@@ -394,8 +398,117 @@ def run_glp(args, ws, rank, local):
         if rank == 0:
             line["batched"] = {k: bl[k] for k in ("metric", "value", "unit", "ms_per_step", "config", "plain",
                                                  "vs_plain", "e2e", "roofline", "cpu_baseline")}
+    if not args.no_served:
+        sv = run_served(args, ws, rank, local)
+        if rank == 0:
+            line["served"] = sv
     if rank == 0:
         print(json.dumps(line))
+
+
+# ----------------------------------------------------------------- served
+def served_requests(count: int, seed: int, device):
+    """The served workload (seed 6): a pool of graphs (24 planted-partition
+    graphs of 10k-100k vertices, R-MAT scales 20-23) and `count` requests
+    over it: 80 % planted / 20 % R-MAT, methods 60 % classic, 25 % layered
+    (3 layers, dstar 2/3/5), 15 % SLPA (T = niter, r = 0.1), niter 10 or 20.
+    Counter based: request i depends only on (seed, i)."""
+    from glp_b200 import graphs
+    from glp_b200.engine import make_params
+    from glp_b200.graphs import _splitmix64
+
+    specs = graphs.batch_specs(24, seed, n_range=(10000, 100000))
+    pool_p = [graphs.planted(s["n"], s["k"], s["intra"], s["inter"], s["seed"], device=device).to("cpu")
+              for s in specs]
+    pool_r = [graphs.rmat(sc, 16, seed=seed * 100 + sc, device=device).to("cpu") for sc in (20, 21, 22, 23)]
+    torch.cuda.empty_cache()
+    pool = pool_p + pool_r
+    reqs = []
+    for i in range(count):
+        u = [_splitmix64(_splitmix64(seed ^ 0xABCDEF) ^ (i * 8 + j)) / 2.0 ** 64 for j in range(6)]
+        g = pool_p[int(u[1] * len(pool_p))] if u[0] < 0.8 else pool_r[int(u[1] * len(pool_r))]
+        niter = 10 if u[3] < 0.5 else 20
+        if u[2] < 0.60:
+            method, params = 1, None
+        elif u[2] < 0.85:
+            method, params = 2, make_params(dstar=[2, 3, 5])
+        else:
+            method, params = 3, make_params(slpa_T=niter, slpa_r=0.1, seed=seed)
+        reqs.append({"g": g, "gi": next(k for k, x in enumerate(pool) if x is g), "method": method, "niter": niter,
+                     "params": params, "u_gap": u[4]})
+    return reqs, pool
+
+
+def _pct(x, q):
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def run_served(args, ws, rank, local):
+    """Open-loop Poisson arrivals at each rate; the native server (continuous
+    batching into the persistent kernel + overlapping one-graph solves)
+    against a sequential one-request-at-a-time engine on the same schedule.
+    Latency = completion - scheduled arrival."""
+    from glp_b200.engine import Graph
+    from glp_b200.server import Server
+
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    t0 = time.time()
+    reqs, pool = served_requests(args.requests, args.serve_seed, dev)
+    gen_s = time.time() - t0
+    rates = [float(x) for x in args.rates.split(",") if x]
+    out = []
+    for rate in rates:
+        arrivals = np.cumsum([-np.log(max(1e-12, 1.0 - r["u_gap"])) / rate for r in reqs])
+        arrivals -= arrivals[0]
+        # served: the pool is resident (uploaded before the stream starts)
+        with Server() as srv:
+            gids = [srv.add_graph(g) for g in pool]
+            handles, lags = [], []
+            start = time.perf_counter()
+            for r, at in zip(reqs, arrivals):
+                wait = start + at - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                lags.append(time.perf_counter() - (start + at))
+                handles.append(srv.submit_graph(gids[r["gi"]], r["method"], r["niter"], r["params"]))
+            stats = [srv.wait(h) for h in handles]
+            rounds = srv.info()["rounds"]
+        lat = [(st["done_s"] - st["submit_s"] + lag) * 1e3 for st, lag in zip(stats, lags)]
+        span = max(st["done_s"] for st in stats) - min(st["submit_s"] for st in stats)
+        served = {"throughput": round(len(reqs) / span, 1), "p50_ms": round(_pct(lat, 50), 2),
+                  "p99_ms": round(_pct(lat, 99), 2), "rounds": int(rounds),
+                  "batched_frac": round(sum(st["path"] == 1 for st in stats) / len(stats), 3)}
+        # sequential one-request-at-a-time engine, same schedule, the same
+        # graphs resident (one handle each, created before the stream)
+        lat_s, same = [], True
+        resident = [Graph(g) for g in pool]
+        start = time.perf_counter()
+        for r, at, h in zip(reqs, arrivals, handles):
+            wait = start + at - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            lab = resident[r["gi"]].run(r["method"], r["niter"], r["params"]).labels
+            lat_s.append((time.perf_counter() - (start + at)) * 1e3)
+            same = same and bool(np.array_equal(lab, h.labels))
+        span_s = (time.perf_counter() - start)
+        for gh in resident:
+            gh.close()
+        seq = {"throughput": round(len(reqs) / span_s, 1), "p50_ms": round(_pct(lat_s, 50), 2),
+               "p99_ms": round(_pct(lat_s, 99), 2)}
+        out.append({"rate": rate, "served": served, "sequential": seq,
+                    "throughput_vs_sequential": round(served["throughput"] / seq["throughput"], 2),
+                    "labels_match_alone": same})
+    mix = {"planted": round(sum(r["g"].n <= 100000 for r in reqs) / len(reqs), 3),
+           "classic": round(sum(r["method"] == 1 for r in reqs) / len(reqs), 3),
+           "layered": round(sum(r["method"] == 2 for r in reqs) / len(reqs), 3),
+           "slpa": round(sum(r["method"] == 3 for r in reqs) / len(reqs), 3)}
+    return {"metric": "served LP throughput (req/s) and p50/p99 latency, open-loop Poisson arrivals",
+            "unit": "req/s", "requests": len(reqs), "seed": args.serve_seed, "mix": mix, "rates": out,
+            "graph_gen_s": round(gen_s, 2),
+            "how": "native server, graph pool resident: FIFO admission by a 150 GB HBM budget, small classic "
+                   "requests in rounds of the persistent batched kernel, the rest on one one-graph worker (shortest job "
+                   "first) with cached "
+                   "handles; sequential = one request at a time through glp_run on resident handles"}
 
 
 # ----------------------------------------------------------------- batched
@@ -544,6 +657,10 @@ def main():
         run_reference(args, ws, rank)
     elif args.workload == "batched":
         res = run_batched(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(res))
+    elif args.workload == "served":
+        res = run_served(args, ws, rank, local)
         if rank == 0:
             print(json.dumps(res))
     else:

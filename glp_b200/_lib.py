@@ -110,11 +110,30 @@ SIGNATURES = {
     "glp_free_host": (None, [C.c_void_p]),
     "glp_batch_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                    C.POINTER(C.c_void_p)]),
+    "glp_batch_create_ex": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                      C.c_void_p, C.POINTER(C.c_void_p)]),
+    "glp_batch_repack": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                   C.c_void_p]),
     "glp_batch_destroy": (None, [C.c_void_p]),
     "glp_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                  C.POINTER(C.c_int32)]),
     "glp_batch_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "glp_batch_tune": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "glp_server_config_default": (C.c_int, [C.c_void_p]),
+    "glp_server_start": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "glp_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32,
+                                    C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int64)]),
+    "glp_server_add_graph": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64,
+                                       C.c_int32, C.POINTER(C.c_int64)]),
+    "glp_server_submit_graph": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                          C.POINTER(C.c_int64)]),
+    "glp_server_remove_graph": (C.c_int, [C.c_void_p, C.c_int64]),
+    "glp_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p]),
+    "glp_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
+    "glp_server_release": (C.c_int, [C.c_void_p, C.c_int64]),
+    "glp_server_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                  C.POINTER(C.c_int64)]),
+    "glp_server_stop": (C.c_int, [C.c_void_p]),
     "glp_run_classic_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p,
                                           C.c_void_p, C.c_void_p]),
 }

@@ -40,6 +40,7 @@
 
 #include "../../include/glp.h"
 #include "device.cuh"
+#include "smem_attr.h"
 
 namespace glp {
 void set_error(const char* fmt, ...);
@@ -67,7 +68,10 @@ struct BatchArgs {
   const int64_t* vbase;    // [G+1]
   int32_t ngraphs;
   int32_t n;               // N
-  int64_t bstart[9];       // bucket q occupies order[bstart[q], bstart[q+1])
+  int32_t nclass;          // iteration classes (graphs grouped by iteration count)
+  int32_t class_niter[8];  // iterations of each class in this run
+  int64_t class_v[9];      // class c owns vertices [class_v[c], class_v[c+1])
+  int64_t bstart[8][9];    // class c, bucket q: order[bstart[c][q], bstart[c][q+1])
   uint32_t mode;           // kB* strategy bits
   uint32_t warp_words;     // shared words per warp for group tables
   uint32_t blk_cap;        // table slots of the block tier
@@ -375,13 +379,17 @@ __global__ void __launch_bounds__(NT) k_batch(BatchArgs a) {
         chg += nxt != own;
       }
       a.lab1[v] = nxt;
+      if (nxt != own) {  // count it only for graphs that run a step
+        int c = 0;
+        while (c + 1 < a.nclass && v >= a.class_v[c + 1]) ++c;
+        if (a.class_niter[c] == 0) --chg;
+      }
     }
     if (a.first_step && a.niter > 0) block_count_add<NT>(a.changed, chg, red_u);
   }
   if (!grid_barrier(a.bar, ++phase * gridDim.x, a.err)) return;
 
   uint32_t* smem_warp = smem + (size_t)warp * a.warp_words;
-  const int64_t* B = a.bstart;
   for (int32_t it = a.first_step ? 1 : 0; it < a.niter; ++it) {
     const int32_t* lin = (it & 1) ? a.lab1 : a.lab0;
     int32_t* lout = (it & 1) ? a.lab0 : a.lab1;
@@ -390,17 +398,21 @@ __global__ void __launch_bounds__(NT) k_batch(BatchArgs a) {
     const bool majority =
         it > 0 && *(volatile unsigned long long*)(a.changed + it - 1) < (unsigned long long)(a.n / 4);
     uint32_t chg = 0;
-    for (int64_t i = B[0] + blockIdx.x; i < B[1]; i += gridDim.x)
-      chg += block_vertex<NT>(a, a.order[i], lin, lout, smem, red) ? 1u : 0u;
-    chg += sweep_groups<NT, 32, 8>(a, B[1], B[2], lin, lout, smem_warp, majority);
-    chg += sweep_groups<NT, 32, 4>(a, B[2], B[3], lin, lout, smem_warp, majority);
-    if (a.mode & kB3Half) chg += sweep_groups<NT, 16, 4>(a, B[3], B[4], lin, lout, smem_warp, majority);
-    else chg += sweep_groups<NT, 32, 2>(a, B[3], B[4], lin, lout, smem_warp, majority);
-    if (a.mode & kB4Threads) chg += sweep_threads<NT, 32>(a, B[4], B[5], lin, lout);
-    else chg += sweep_groups<NT, 8, 4>(a, B[4], B[5], lin, lout, smem_warp, majority);
-    if (a.mode & kB5Threads) chg += sweep_threads<NT, 16>(a, B[5], B[6], lin, lout);
-    else chg += sweep_groups<NT, 4, 4>(a, B[5], B[6], lin, lout, smem_warp, majority);
-    chg += sweep_threads<NT, 8>(a, B[6], B[7], lin, lout);
+    for (int c = 0; c < a.nclass; ++c) {
+      if (it >= a.class_niter[c]) continue;  // this class has finished
+      const int64_t* B = a.bstart[c];
+      for (int64_t i = B[0] + blockIdx.x; i < B[1]; i += gridDim.x)
+        chg += block_vertex<NT>(a, a.order[i], lin, lout, smem, red) ? 1u : 0u;
+      chg += sweep_groups<NT, 32, 8>(a, B[1], B[2], lin, lout, smem_warp, majority);
+      chg += sweep_groups<NT, 32, 4>(a, B[2], B[3], lin, lout, smem_warp, majority);
+      if (a.mode & kB3Half) chg += sweep_groups<NT, 16, 4>(a, B[3], B[4], lin, lout, smem_warp, majority);
+      else chg += sweep_groups<NT, 32, 2>(a, B[3], B[4], lin, lout, smem_warp, majority);
+      if (a.mode & kB4Threads) chg += sweep_threads<NT, 32>(a, B[4], B[5], lin, lout);
+      else chg += sweep_groups<NT, 8, 4>(a, B[4], B[5], lin, lout, smem_warp, majority);
+      if (a.mode & kB5Threads) chg += sweep_threads<NT, 16>(a, B[5], B[6], lin, lout);
+      else chg += sweep_groups<NT, 4, 4>(a, B[5], B[6], lin, lout, smem_warp, majority);
+      chg += sweep_threads<NT, 8>(a, B[6], B[7], lin, lout);
+    }
     block_count_add<NT>(a.changed + it, chg, red_u);
     if (it + 1 < a.niter && !grid_barrier(a.bar, ++phase * gridDim.x, a.err)) return;
   }
@@ -474,49 +486,61 @@ __host__ __device__ __forceinline__ int bucket_of(int32_t d) {
   return d > 256 ? 0 : d > 128 ? 1 : d > 64 ? 2 : d > 32 ? 3 : d > 16 ? 4 : d > 8 ? 5 : d > 0 ? 6 : 7;
 }
 constexpr int kOrderChunk = 2048;  // vertices per block in the two passes below
+constexpr int kMaxClasses = 8;     // distinct iteration counts in one batch
+constexpr int kKeys = kMaxClasses * kBuckets;
 
-// Pass 1: per block (a chunk of kOrderChunk consecutive vertices) the number
-// of its vertices in each bucket.
-__global__ void __launch_bounds__(256) k_order_count(const int64_t* __restrict__ off, int64_t n,
-                                                     uint32_t* __restrict__ counts) {
-  __shared__ uint32_t c[kBuckets];
-  if (threadIdx.x < kBuckets) c[threadIdx.x] = 0;
-  __syncthreads();
-  const int64_t v0 = (int64_t)blockIdx.x * kOrderChunk;
-  for (int64_t v = v0 + threadIdx.x; v < n && v < v0 + kOrderChunk; v += 256)
-    atomicAdd(&c[bucket_of((int32_t)(off[v + 1] - off[v]))], 1u);
-  __syncthreads();
-  if (threadIdx.x < kBuckets) counts[(size_t)blockIdx.x * kBuckets + threadIdx.x] = c[threadIdx.x];
+struct ClassRanges {
+  int64_t vstart[kMaxClasses + 1];  // class c owns vertices [vstart[c], vstart[c+1])
+  int32_t nclass;
+};
+__device__ __forceinline__ int class_of(const ClassRanges& cr, int64_t v) {
+  int c = 0;
+  while (c + 1 < cr.nclass && v >= cr.vstart[c + 1]) ++c;
+  return c;
+}
+__device__ __forceinline__ int order_key(const int64_t* __restrict__ off, const ClassRanges& cr, int64_t v) {
+  return class_of(cr, v) * kBuckets + bucket_of((int32_t)(off[v + 1] - off[v]));
 }
 
-// Pass 2: each block places its vertices at start[block][bucket] onwards in
-// id order (ranks from warp ballots and a running count per bucket).
-__global__ void __launch_bounds__(256) k_order_scatter(const int64_t* __restrict__ off, int64_t n,
+// Pass 1: per block (a chunk of kOrderChunk consecutive vertices) the number
+// of its vertices under each (class, bucket) key.
+__global__ void __launch_bounds__(256) k_order_count(const int64_t* __restrict__ off, int64_t n, ClassRanges cr,
+                                                     uint32_t* __restrict__ counts) {
+  __shared__ uint32_t c[kKeys];
+  if (threadIdx.x < kKeys) c[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t v0 = (int64_t)blockIdx.x * kOrderChunk;
+  for (int64_t v = v0 + threadIdx.x; v < n && v < v0 + kOrderChunk; v += 256) atomicAdd(&c[order_key(off, cr, v)], 1u);
+  __syncthreads();
+  if (threadIdx.x < kKeys) counts[(size_t)blockIdx.x * kKeys + threadIdx.x] = c[threadIdx.x];
+}
+
+// Pass 2: each block places its vertices at start[block][key] onwards in id
+// order (ranks inside a warp from __match_any_sync, then by warp).
+__global__ void __launch_bounds__(256) k_order_scatter(const int64_t* __restrict__ off, int64_t n, ClassRanges cr,
                                                        const int64_t* __restrict__ start,
                                                        int32_t* __restrict__ order) {
-  __shared__ uint32_t wc[8][kBuckets];  // per warp, per bucket
-  __shared__ int64_t run[kBuckets];
+  __shared__ uint32_t wc[8][kKeys];  // per warp, per key
+  __shared__ int64_t run[kKeys];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x < kBuckets) run[threadIdx.x] = start[(size_t)blockIdx.x * kBuckets + threadIdx.x];
+  if (threadIdx.x < kKeys) run[threadIdx.x] = start[(size_t)blockIdx.x * kKeys + threadIdx.x];
   const int64_t v0 = (int64_t)blockIdx.x * kOrderChunk;
   for (int64_t s0 = v0; s0 < v0 + kOrderChunk && s0 < n; s0 += 256) {
-    const int64_t v = s0 + threadIdx.x;
-    const int bk = v < n ? bucket_of((int32_t)(off[v + 1] - off[v])) : -1;
-    uint32_t rank = 0;
-#pragma unroll
-    for (int q = 0; q < kBuckets; ++q) {
-      const uint32_t m = __ballot_sync(kFull, bk == q);
-      if (lane == 0) wc[warp][q] = __popc(m);
-      if (bk == q) rank = __popc(m & ((1u << lane) - 1u));
-    }
+    for (int i = threadIdx.x; i < 8 * kKeys; i += 256) (&wc[0][0])[i] = 0;
     __syncthreads();
-    if (bk >= 0) {
-      int64_t pos = run[bk] + rank;
-      for (int w = 0; w < warp; ++w) pos += wc[w][bk];
+    const int64_t v = s0 + threadIdx.x;
+    const int key = v < n ? order_key(off, cr, v) : -1;
+    const uint32_t peers = __match_any_sync(kFull, key);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    if (key >= 0 && rank == 0) wc[warp][key] = __popc(peers);
+    __syncthreads();
+    if (key >= 0) {
+      int64_t pos = run[key] + rank;
+      for (int w = 0; w < warp; ++w) pos += wc[w][key];
       order[pos] = (int32_t)v;
     }
     __syncthreads();
-    if (threadIdx.x < kBuckets) {
+    if (threadIdx.x < kKeys) {
       uint32_t t = 0;
       for (int w = 0; w < 8; ++w) t += wc[w][threadIdx.x];
       run[threadIdx.x] += t;
@@ -545,8 +569,23 @@ struct glp_batch {
   int32_t* d_cols = nullptr;
   int32_t* d_order = nullptr;
   int64_t* d_vbase = nullptr;
+  int64_t* d_ebase = nullptr;
+  int32_t* d_stage = nullptr;        // staged local offsets
+  uint32_t* d_counts = nullptr;      // per-block (class, bucket) counts
+  int64_t* d_start = nullptr;        // per-block (class, bucket) starts
+  unsigned long long* d_hist = nullptr;
+  uint32_t* d_flags = nullptr;
+  size_t cap_off = 0, cap_cols = 0, cap_order = 0, cap_vbase = 0, cap_ebase = 0, cap_stage = 0, cap_counts = 0,
+         cap_start = 0, cap_lab[2] = {0, 0};
+  std::vector<uint32_t> h_counts;
+  std::vector<int64_t> h_starts;
   std::vector<int64_t> h_vbase, h_ebase;
   std::vector<unsigned long long> hist;  // vertices per degree 0..kBatchMaxDegree
+  // iteration classes: graphs with equal iteration counts, contiguous
+  int32_t nclass = 1;
+  int32_t class_niter[8] = {0};
+  int64_t class_v[9] = {0};
+  int64_t bstart[8][9] = {{0}};
   int32_t* d_lab[2] = {nullptr, nullptr};
   unsigned long long* d_changed = nullptr;
   int32_t changed_cap = 0;
@@ -582,7 +621,7 @@ int max_degree_in(const glp_batch* b, int lo, int hi) {  // largest degree d wit
 template <int NT>
 int launch_k(glp_batch* b, const BatchArgs& a, size_t smem, cudaStream_t s) {
   auto kern = k_batch<NT>;
-  GLP_BCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GLP_BCUDA(raise_smem_limit((const void*)kern, smem));
   int per_sm = 0;
   GLP_BCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
   if (per_sm < 1) {
@@ -611,6 +650,15 @@ int launch_cfg(glp_batch* b, const Config& c, const BatchArgs& a, cudaStream_t s
   return GLP_EINVAL;
 }
 
+// niter >= 0: every graph runs niter iterations; GLP_BATCH_OWN_ITERATIONS:
+// each graph runs the count it was created with.
+int32_t run_niter(const glp_batch* b, int32_t niter, int c) { return niter >= 0 ? niter : b->class_niter[c]; }
+int32_t max_niter(const glp_batch* b, int32_t niter) {
+  int32_t mx = 0;
+  for (int c = 0; c < b->nclass; ++c) mx = std::max(mx, run_niter(b, niter, c));
+  return mx;
+}
+
 BatchArgs make_args(glp_batch* b, const Config& c, int32_t niter) {
   BatchArgs a{};
   a.off = b->d_off;
@@ -619,17 +667,14 @@ BatchArgs make_args(glp_batch* b, const Config& c, int32_t niter) {
   a.vbase = b->d_vbase;
   a.ngraphs = b->ngraphs;
   a.n = (int32_t)b->n;
-  // bucket q holds the degrees of bucket_of() == q, in that order
-  static const int kLo[kBuckets] = {256, 128, 64, 32, 16, 8, 0, -1};
-  static const int kHi[kBuckets] = {kBatchMaxDegree, 256, 128, 64, 32, 16, 8, 0};
-  a.bstart[0] = 0;
-  for (int q = 0; q < kBuckets; ++q) {
-    int64_t cnt = 0;
-    for (int d = kLo[q] + 1; d <= kHi[q]; ++d) cnt += (int64_t)b->hist[d];
-    a.bstart[q + 1] = a.bstart[q] + cnt;
+  a.nclass = b->nclass;
+  for (int k = 0; k < b->nclass; ++k) {
+    a.class_niter[k] = run_niter(b, niter, k);
+    for (int q = 0; q <= kBuckets; ++q) a.bstart[k][q] = b->bstart[k][q];
   }
+  for (int k = 0; k <= b->nclass; ++k) a.class_v[k] = b->class_v[k];
   a.mode = (c.tt >= 32 ? kB4Threads : 0u) | (c.tt >= 16 ? kB5Threads : 0u) | (c.half ? kB3Half : 0u);
-  a.warp_words = a.bstart[2] > a.bstart[1] ? 2 * group_slots<32, 8>() : 2 * group_slots<32, 4>();
+  a.warp_words = max_degree_in(b, 128, 256) ? 2 * group_slots<32, 8>() : 2 * group_slots<32, 4>();
   const int bdeg = max_degree_in(b, 256, kBatchMaxDegree);
   a.blk_cap = bdeg ? pow2_host(2u * (uint32_t)bdeg) : 0u;
   a.lab0 = b->d_lab[0];
@@ -637,7 +682,7 @@ BatchArgs make_args(glp_batch* b, const Config& c, int32_t niter) {
   a.changed = b->d_changed;
   a.bar = b->d_bar;
   a.err = b->d_err;
-  a.niter = niter;
+  a.niter = max_niter(b, niter);
   a.first_step = b->first_step;
   return a;
 }
@@ -655,7 +700,7 @@ int ensure_changed(glp_batch* b, int32_t niter) {
 // Enqueues one whole run (reset of counters and barrier, the persistent
 // launch) on s.
 int enqueue_run(glp_batch* b, const Config& c, int32_t niter, cudaStream_t s) {
-  GLP_BCUDA(cudaMemsetAsync(b->d_changed, 0, sizeof(unsigned long long) * std::max(niter, 1), s));
+  GLP_BCUDA(cudaMemsetAsync(b->d_changed, 0, sizeof(unsigned long long) * std::max(max_niter(b, niter), 1), s));
   GLP_BCUDA(cudaMemsetAsync(b->d_bar, 0, sizeof(unsigned int), s));
   GLP_BCUDA(cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), s));
   if (b->n == 0) return GLP_OK;
@@ -694,38 +739,22 @@ void free_graph_exec(glp_batch* b) {
   b->g_niter = -1;
 }
 
-}  // namespace
-}  // namespace glp
+// Grow-only device buffer: reallocated only when a larger one is needed, so
+// repacking a batch allocates nothing once it has seen its largest round.
+template <class T>
+int grow(T** p, size_t* cap, size_t need) {
+  need = std::max<size_t>(need, 1);
+  if (*p && *cap >= need) return GLP_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t want = need + need / 4;
+  GLP_BCUDA(cudaMalloc(p, sizeof(T) * want));
+  *cap = want;
+  return GLP_OK;
+}
 
-using namespace glp;
-
-extern "C" {
-
-int glp_batch_create(int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols, const int32_t* n,
-                     const int64_t* m, int32_t on_device, glp_batch** out) {
-  if (!out || ngraphs < 0 || (ngraphs > 0 && (!offsets || !cols || !n || !m))) {
-    set_error("bad batch arguments");
-    return GLP_EINVAL;
-  }
-  *out = nullptr;
-  std::unique_ptr<glp_batch> b(new glp_batch());
-  b->ngraphs = ngraphs;
-  b->h_vbase.assign((size_t)ngraphs + 1, 0);
-  b->h_ebase.assign((size_t)ngraphs + 1, 0);
-  for (int32_t g = 0; g < ngraphs; ++g) {
-    if (n[g] < 0 || m[g] < 0 || !offsets[g] || (m[g] > 0 && !cols[g])) {
-      set_error("graph %d: bad arguments (n=%d, m=%lld)", g, n[g], (long long)m[g]);
-      return GLP_EINVAL;
-    }
-    b->h_vbase[g + 1] = b->h_vbase[g] + n[g];
-    b->h_ebase[g + 1] = b->h_ebase[g] + m[g];
-  }
-  b->n = b->h_vbase[ngraphs];
-  b->m = b->h_ebase[ngraphs];
-  if (b->n >= INT32_MAX || b->m >= INT32_MAX * 64ll) {
-    set_error("batch of %lld vertices / %lld entries exceeds the packed layout", (long long)b->n, (long long)b->m);
-    return GLP_EINVAL;
-  }
+int init_device(glp_batch* b) {
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
@@ -741,41 +770,96 @@ int glp_batch_create(int32_t ngraphs, const int32_t* const* offsets, const int32
     return GLP_ENOTSUP;
   }
   GLP_BCUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  cudaStream_t s = b->stream;
-  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  GLP_BCUDA(cudaMalloc(&b->d_off, sizeof(int64_t) * (size_t)(b->n + 1)));
-  GLP_BCUDA(cudaMalloc(&b->d_cols, sizeof(int32_t) * (size_t)std::max<int64_t>(b->m, 1)));
-  GLP_BCUDA(cudaMalloc(&b->d_order, sizeof(int32_t) * (size_t)std::max<int64_t>(b->n, 1)));
-  GLP_BCUDA(cudaMalloc(&b->d_vbase, sizeof(int64_t) * (size_t)(ngraphs + 1)));
-  GLP_BCUDA(cudaMalloc(&b->d_lab[0], sizeof(int32_t) * (size_t)std::max<int64_t>(b->n, 1)));
-  GLP_BCUDA(cudaMalloc(&b->d_lab[1], sizeof(int32_t) * (size_t)std::max<int64_t>(b->n, 1)));
   GLP_BCUDA(cudaMalloc(&b->d_bar, sizeof(unsigned int)));
   GLP_BCUDA(cudaMalloc(&b->d_err, sizeof(uint32_t)));
-  if (ensure_changed(b.get(), 32)) return GLP_ENOMEM;
-  // staging: local offsets of graph g at [vbase_g + g, vbase_g + g + n_g]
-  int32_t* stage = nullptr;
-  int64_t* d_ebase = nullptr;
-  unsigned long long* d_hist = nullptr;
-  uint32_t* d_flags = nullptr;
-  auto cleanup = [&]() {
-    cudaFree(stage);
-    cudaFree(d_ebase);
-    cudaFree(d_hist);
-    cudaFree(d_flags);
+  GLP_BCUDA(cudaMalloc(&b->d_flags, sizeof(uint32_t)));
+  GLP_BCUDA(cudaMalloc(&b->d_hist, sizeof(unsigned long long) * (kBatchMaxDegree + 1)));
+  return ensure_changed(b, 32);
+}
+
+// (Re)packs the graphs into b's buffers and builds the work order.
+int pack(glp_batch* b, int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols, const int32_t* n,
+         const int64_t* m, int32_t on_device, const int32_t* niter) {
+  if (ngraphs < 0 || (ngraphs > 0 && (!offsets || !cols || !n || !m))) {
+    set_error("bad batch arguments");
+    return GLP_EINVAL;
+  }
+  b->ngraphs = ngraphs;
+  b->n = b->m = 0;
+  b->h_vbase.assign((size_t)ngraphs + 1, 0);
+  b->h_ebase.assign((size_t)ngraphs + 1, 0);
+  for (int32_t g = 0; g < ngraphs; ++g) {
+    if (n[g] < 0 || m[g] < 0 || !offsets[g] || (m[g] > 0 && !cols[g])) {
+      set_error("graph %d: bad arguments (n=%d, m=%lld)", g, n[g], (long long)m[g]);
+      b->ngraphs = 0;
+      return GLP_EINVAL;
+    }
+    b->h_vbase[g + 1] = b->h_vbase[g] + n[g];
+    b->h_ebase[g + 1] = b->h_ebase[g] + m[g];
+  }
+  const int64_t N = b->h_vbase[ngraphs], M = b->h_ebase[ngraphs];
+  if (N >= INT32_MAX) {
+    set_error("batch of %lld vertices exceeds the packed layout", (long long)N);
+    b->ngraphs = 0;
+    return GLP_EINVAL;
+  }
+  // iteration classes: runs of equal counts (graphs sorted by count)
+  b->nclass = 1;
+  b->class_v[0] = 0;
+  b->class_niter[0] = 0;
+  if (niter) {
+    for (int32_t g = 0; g < ngraphs; ++g) {
+      if (niter[g] < 0 || (g > 0 && niter[g] < niter[g - 1])) {
+        set_error("per-graph iteration counts must be >= 0 and non-decreasing (graph %d)", g);
+        b->ngraphs = 0;
+        return GLP_EINVAL;
+      }
+      if (g == 0) {
+        b->class_niter[0] = niter[0];
+      } else if (niter[g] != niter[g - 1]) {
+        if (b->nclass == kMaxClasses) {
+          set_error("more than %d distinct iteration counts in one batch", kMaxClasses);
+          b->ngraphs = 0;
+          return GLP_ENOTSUP;
+        }
+        b->class_v[b->nclass] = b->h_vbase[g];
+        b->class_niter[b->nclass++] = niter[g];
+      }
+    }
+  }
+  b->class_v[b->nclass] = N;
+  int rc;
+  const int64_t nblocks = std::max<int64_t>((N + kOrderChunk - 1) / kOrderChunk, 1);
+  if ((rc = grow(&b->d_off, &b->cap_off, (size_t)N + 1)) || (rc = grow(&b->d_cols, &b->cap_cols, (size_t)M)) ||
+      (rc = grow(&b->d_order, &b->cap_order, (size_t)N)) || (rc = grow(&b->d_vbase, &b->cap_vbase, (size_t)ngraphs + 1)) ||
+      (rc = grow(&b->d_ebase, &b->cap_ebase, (size_t)ngraphs + 1)) ||
+      (rc = grow(&b->d_lab[0], &b->cap_lab[0], (size_t)N)) || (rc = grow(&b->d_lab[1], &b->cap_lab[1], (size_t)N)) ||
+      (rc = grow(&b->d_stage, &b->cap_stage, (size_t)(N + ngraphs + 1))) ||
+      (rc = grow(&b->d_counts, &b->cap_counts, (size_t)nblocks * kKeys)) ||
+      (rc = grow(&b->d_start, &b->cap_start, (size_t)nblocks * kKeys))) {
+    b->ngraphs = 0;
+    return rc;
+  }
+  b->n = N;
+  b->m = M;
+  cudaStream_t s = b->stream;
+  auto bad = [&](int code, const char* msg) {
+    set_error("%s", msg);
+    b->ngraphs = 0;
+    b->n = b->m = 0;
+    return code;
   };
+  cudaError_t e;
   auto fail = [&](cudaError_t err, const char* what) {
-    cleanup();
+    b->ngraphs = 0;
+    b->n = b->m = 0;
     return cuda_fail(err, what);
   };
-  if ((e = cudaMalloc(&stage, sizeof(int32_t) * (size_t)(b->n + ngraphs + 1))) != cudaSuccess)
-    return fail(e, "batch staging");
-  if ((e = cudaMalloc(&d_ebase, sizeof(int64_t) * (size_t)(ngraphs + 1))) != cudaSuccess ||
-      (e = cudaMalloc(&d_hist, sizeof(unsigned long long) * (kBatchMaxDegree + 1))) != cudaSuccess ||
-      (e = cudaMalloc(&d_flags, sizeof(uint32_t))) != cudaSuccess)
-    return fail(e, "batch scratch");
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  // staging: local offsets of graph g at [vbase_g + g, vbase_g + g + n_g]
   for (int32_t g = 0; g < ngraphs; ++g) {
-    if ((e = cudaMemcpyAsync(stage + b->h_vbase[g] + g, offsets[g], sizeof(int32_t) * ((size_t)n[g] + 1), kind, s)) !=
-        cudaSuccess)
+    if ((e = cudaMemcpyAsync(b->d_stage + b->h_vbase[g] + g, offsets[g], sizeof(int32_t) * ((size_t)n[g] + 1), kind,
+                             s)) != cudaSuccess)
       return fail(e, "batch offsets copy");
     if (m[g] && (e = cudaMemcpyAsync(b->d_cols + b->h_ebase[g], cols[g], sizeof(int32_t) * (size_t)m[g], kind, s)) !=
                     cudaSuccess)
@@ -783,88 +867,122 @@ int glp_batch_create(int32_t ngraphs, const int32_t* const* offsets, const int32
   }
   if ((e = cudaMemcpyAsync(b->d_vbase, b->h_vbase.data(), sizeof(int64_t) * (ngraphs + 1), cudaMemcpyHostToDevice,
                            s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(d_ebase, b->h_ebase.data(), sizeof(int64_t) * (ngraphs + 1), cudaMemcpyHostToDevice, s)) !=
-          cudaSuccess ||
-      (e = cudaMemsetAsync(d_hist, 0, sizeof(unsigned long long) * (kBatchMaxDegree + 1), s)) != cudaSuccess ||
-      (e = cudaMemsetAsync(d_flags, 0, sizeof(uint32_t), s)) != cudaSuccess)
+      (e = cudaMemcpyAsync(b->d_ebase, b->h_ebase.data(), sizeof(int64_t) * (ngraphs + 1), cudaMemcpyHostToDevice,
+                           s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(b->d_hist, 0, sizeof(unsigned long long) * (kBatchMaxDegree + 1), s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(b->d_flags, 0, sizeof(uint32_t), s)) != cudaSuccess)
     return fail(e, "batch set-up");
   const unsigned grid = (unsigned)std::max(1, b->nsm * 8);
-  if (b->n) k_pack_vertices<<<grid, 256, 0, s>>>(stage, b->d_vbase, d_ebase, ngraphs, b->n, b->d_off, d_hist, d_flags);
-  else if ((e = cudaMemsetAsync(b->d_off, 0, sizeof(int64_t), s)) != cudaSuccess) return fail(e, "batch offsets");
+  if (N)
+    k_pack_vertices<<<grid, 256, 0, s>>>(b->d_stage, b->d_vbase, b->d_ebase, ngraphs, N, b->d_off, b->d_hist,
+                                         b->d_flags);
+  else if ((e = cudaMemsetAsync(b->d_off, 0, sizeof(int64_t), s)) != cudaSuccess)
+    return fail(e, "batch offsets");
   uint32_t flags = 0;
   if ((e = cudaGetLastError()) != cudaSuccess ||
-      (e = cudaMemcpyAsync(&flags, d_flags, sizeof flags, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(&flags, b->d_flags, sizeof flags, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return fail(e, "batch vertex pass");
-  if (flags & kBadOffsets) {
-    cleanup();
-    set_error("a graph's offsets are malformed (offsets[0] = 0, non-decreasing, offsets[n] = m)");
-    return GLP_EINVAL;
-  }
-  if (flags & kBadDegree) {
-    cleanup();
-    set_error("a vertex degree exceeds the batch limit of %d (run that graph through glp_run)", kBatchMaxDegree);
-    return GLP_ENOTSUP;
-  }
-  if (b->m) k_pack_cols<<<grid, 256, 0, s>>>(b->d_cols, b->d_vbase, d_ebase, ngraphs, b->m, d_flags);
-  if (b->n) k_pack_sorted<<<grid, 256, 0, s>>>(b->d_off, b->d_cols, b->n, d_flags);
+  if (flags & kBadOffsets)
+    return bad(GLP_EINVAL, "a graph's offsets are malformed (offsets[0] = 0, non-decreasing, offsets[n] = m)");
+  if (flags & kBadDegree)
+    return bad(GLP_ENOTSUP, "a vertex degree exceeds the batch limit of 4096 (run that graph through glp_run)");
+  if (M) k_pack_cols<<<grid, 256, 0, s>>>(b->d_cols, b->d_vbase, b->d_ebase, ngraphs, M, b->d_flags);
+  if (N) k_pack_sorted<<<grid, 256, 0, s>>>(b->d_off, b->d_cols, N, b->d_flags);
   b->hist.assign(kBatchMaxDegree + 1, 0ull);
   if ((e = cudaGetLastError()) != cudaSuccess ||
-      (e = cudaMemcpyAsync(&flags, d_flags, sizeof flags, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(b->hist.data(), d_hist, sizeof(unsigned long long) * (kBatchMaxDegree + 1),
+      (e = cudaMemcpyAsync(&flags, b->d_flags, sizeof flags, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(b->hist.data(), b->d_hist, sizeof(unsigned long long) * (kBatchMaxDegree + 1),
                            cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return fail(e, "batch edge pass");
-  if (flags & kBadCols) {
-    cleanup();
-    set_error("a column index lies outside its graph's [0, n)");
-    return GLP_EINVAL;
-  }
+  if (flags & kBadCols) return bad(GLP_EINVAL, "a column index lies outside its graph's [0, n)");
   b->first_step = (flags & kUnsortedRow) ? 0 : 1;
+  b->max_degree = 0;
   for (int d = kBatchMaxDegree; d >= 0; --d)
     if (b->hist[d]) {
       b->max_degree = d;
       break;
     }
-  // bucketed work order (two passes, per-block bucket starts from the host)
-  if (b->n) {
-    const int64_t nblocks = (b->n + kOrderChunk - 1) / kOrderChunk;
-    uint32_t* d_counts = nullptr;
-    int64_t* d_start = nullptr;
-    std::vector<uint32_t> counts((size_t)nblocks * kBuckets);
-    std::vector<int64_t> starts((size_t)nblocks * kBuckets);
-    auto fail2 = [&](cudaError_t err, const char* what) {
-      cudaFree(d_counts);
-      cudaFree(d_start);
-      return fail(err, what);
-    };
-    if ((e = cudaMalloc(&d_counts, sizeof(uint32_t) * counts.size())) != cudaSuccess ||
-        (e = cudaMalloc(&d_start, sizeof(int64_t) * starts.size())) != cudaSuccess)
-      return fail2(e, "batch order scratch");
-    k_order_count<<<(unsigned)nblocks, 256, 0, s>>>(b->d_off, b->n, d_counts);
+  // work order (two passes, per-block (class, bucket) starts from the host):
+  // class-major, then bucket-major, then vertex id
+  ClassRanges cr{};
+  cr.nclass = b->nclass;
+  for (int c = 0; c <= b->nclass; ++c) cr.vstart[c] = b->class_v[c];
+  for (int c = 0; c < kMaxClasses; ++c)
+    for (int q = 0; q <= kBuckets; ++q) b->bstart[c][q] = 0;
+  if (N) {
+    std::vector<uint32_t>& counts = b->h_counts;
+    std::vector<int64_t>& starts = b->h_starts;
+    counts.resize((size_t)nblocks * kKeys);
+    starts.resize((size_t)nblocks * kKeys);
+    k_order_count<<<(unsigned)nblocks, 256, 0, s>>>(b->d_off, N, cr, b->d_counts);
     if ((e = cudaGetLastError()) != cudaSuccess ||
-        (e = cudaMemcpyAsync(counts.data(), d_counts, sizeof(uint32_t) * counts.size(), cudaMemcpyDeviceToHost,
+        (e = cudaMemcpyAsync(counts.data(), b->d_counts, sizeof(uint32_t) * counts.size(), cudaMemcpyDeviceToHost,
                              s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
-      return fail2(e, "batch order count");
+      return fail(e, "batch order count");
     int64_t acc = 0;
-    for (int q = 0; q < kBuckets; ++q)
+    for (int key = 0; key < kKeys; ++key) {
+      const int c = key / kBuckets, q = key % kBuckets;
+      if (c < b->nclass) b->bstart[c][q] = acc;
       for (int64_t k = 0; k < nblocks; ++k) {
-        starts[(size_t)k * kBuckets + q] = acc;
-        acc += counts[(size_t)k * kBuckets + q];
+        starts[(size_t)k * kKeys + key] = acc;
+        acc += counts[(size_t)k * kKeys + key];
       }
-    if ((e = cudaMemcpyAsync(d_start, starts.data(), sizeof(int64_t) * starts.size(), cudaMemcpyHostToDevice, s)) !=
+      if (c < b->nclass) b->bstart[c][q + 1] = acc;
+    }
+    if ((e = cudaMemcpyAsync(b->d_start, starts.data(), sizeof(int64_t) * starts.size(), cudaMemcpyHostToDevice, s)) !=
         cudaSuccess)
-      return fail2(e, "batch order starts");
-    k_order_scatter<<<(unsigned)nblocks, 256, 0, s>>>(b->d_off, b->n, d_start, b->d_order);
+      return fail(e, "batch order starts");
+    k_order_scatter<<<(unsigned)nblocks, 256, 0, s>>>(b->d_off, N, cr, b->d_start, b->d_order);
     if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
-      return fail2(e, "batch order scatter");
-    cudaFree(d_counts);
-    cudaFree(d_start);
+      return fail(e, "batch order scatter");
   }
-  cleanup();
+  return GLP_OK;
+}
+
+}  // namespace
+}  // namespace glp
+
+using namespace glp;
+
+extern "C" {
+
+int glp_batch_create(int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols, const int32_t* n,
+                     const int64_t* m, int32_t on_device, glp_batch** out) {
+  return glp_batch_create_ex(ngraphs, offsets, cols, n, m, on_device, nullptr, out);
+}
+
+int glp_batch_create_ex(int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols, const int32_t* n,
+                        const int64_t* m, int32_t on_device, const int32_t* niter, glp_batch** out) {
+  if (!out) {
+    set_error("out is NULL");
+    return GLP_EINVAL;
+  }
+  *out = nullptr;
+  std::unique_ptr<glp_batch> b(new glp_batch());
+  int rc = init_device(b.get());
+  if (rc) {
+    glp_batch_destroy(b.release());
+    return rc;
+  }
+  if ((rc = pack(b.get(), ngraphs, offsets, cols, n, m, on_device, niter))) {
+    glp_batch_destroy(b.release());
+    return rc;
+  }
   *out = b.release();
   return GLP_OK;
+}
+
+int glp_batch_repack(glp_batch* b, int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols,
+                     const int32_t* n, const int64_t* m, int32_t on_device, const int32_t* niter) {
+  if (!b) {
+    set_error("batch is NULL");
+    return GLP_EINVAL;
+  }
+  free_graph_exec(b);
+  return pack(b, ngraphs, offsets, cols, n, m, on_device, niter);
 }
 
 void glp_batch_destroy(glp_batch* b) {
@@ -874,6 +992,12 @@ void glp_batch_destroy(glp_batch* b) {
   cudaFree(b->d_cols);
   cudaFree(b->d_order);
   cudaFree(b->d_vbase);
+  cudaFree(b->d_ebase);
+  cudaFree(b->d_stage);
+  cudaFree(b->d_counts);
+  cudaFree(b->d_start);
+  cudaFree(b->d_hist);
+  cudaFree(b->d_flags);
   cudaFree(b->d_lab[0]);
   cudaFree(b->d_lab[1]);
   cudaFree(b->d_changed);
@@ -897,7 +1021,7 @@ int glp_batch_info(const glp_batch* b, int64_t* n, int64_t* m, int32_t* max_degr
 
 int glp_batch_run(glp_batch* b, const glp_params* p, int32_t niter, int32_t* labels, int32_t on_device,
                   int64_t* changed, void* stream) {
-  if (!b || niter < 0 || (!labels && b->n > 0)) {
+  if (!b || niter < GLP_BATCH_OWN_ITERATIONS || (!labels && b->n > 0)) {
     set_error("bad arguments to glp_batch_run");
     return GLP_EINVAL;
   }
@@ -907,8 +1031,20 @@ int glp_batch_run(glp_batch* b, const glp_params* p, int32_t niter, int32_t* lab
   }
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
   const Config c = config_from(b, p);
-  int rc = ensure_changed(b, niter);
+  const int32_t total = max_niter(b, niter);
+  int rc = ensure_changed(b, total);
   if (rc) return rc;
+  // graph g's labels end in the buffer of its iteration count's parity
+  auto copy_out = [&](cudaMemcpyKind kind) -> cudaError_t {
+    for (int k = 0; k < b->nclass; ++k) {
+      const int64_t lo = b->class_v[k], hi = b->class_v[k + 1];
+      if (hi <= lo) continue;
+      const int32_t* src = b->d_lab[run_niter(b, niter, k) & 1];
+      const cudaError_t e = cudaMemcpyAsync(labels + lo, src + lo, sizeof(int32_t) * (size_t)(hi - lo), kind, s);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
   const bool use_graph = p && p->use_graph;
   if (use_graph) {
     const bool hit = b->gexec && b->g_niter == niter && b->g_cfg == c && b->g_stream == s &&
@@ -918,11 +1054,7 @@ int glp_batch_run(glp_batch* b, const glp_params* p, int32_t niter, int32_t* lab
       cudaGraph_t graph = nullptr;
       GLP_BCUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       rc = enqueue_run(b, c, niter, s);
-      if (!rc && on_device && b->n)
-        rc = cudaMemcpyAsync(labels, b->d_lab[niter & 1], sizeof(int32_t) * (size_t)b->n, cudaMemcpyDeviceToDevice,
-                             s) == cudaSuccess
-                 ? GLP_OK
-                 : GLP_ECUDA;
+      if (!rc && on_device && b->n) rc = copy_out(cudaMemcpyDeviceToDevice) == cudaSuccess ? GLP_OK : GLP_ECUDA;
       const cudaError_t ee = cudaStreamEndCapture(s, &graph);
       if (rc) {
         if (graph) cudaGraphDestroy(graph);
@@ -943,17 +1075,14 @@ int glp_batch_run(glp_batch* b, const glp_params* p, int32_t niter, int32_t* lab
     GLP_BCUDA(cudaGraphLaunch(b->gexec, s));
   } else {
     if ((rc = enqueue_run(b, c, niter, s))) return rc;
-    if (on_device && b->n)
-      GLP_BCUDA(cudaMemcpyAsync(labels, b->d_lab[niter & 1], sizeof(int32_t) * (size_t)b->n,
-                                cudaMemcpyDeviceToDevice, s));
+    if (on_device && b->n) GLP_BCUDA(copy_out(cudaMemcpyDeviceToDevice));
   }
-  if (!on_device && b->n)
-    GLP_BCUDA(cudaMemcpyAsync(labels, b->d_lab[niter & 1], sizeof(int32_t) * (size_t)b->n, cudaMemcpyDeviceToHost, s));
-  if (changed && niter) {
-    std::vector<unsigned long long> tmp((size_t)niter);
-    GLP_BCUDA(cudaMemcpyAsync(tmp.data(), b->d_changed, sizeof(unsigned long long) * niter, cudaMemcpyDeviceToHost, s));
+  if (!on_device && b->n) GLP_BCUDA(copy_out(cudaMemcpyDeviceToHost));
+  if (changed && total) {
+    std::vector<unsigned long long> tmp((size_t)total);
+    GLP_BCUDA(cudaMemcpyAsync(tmp.data(), b->d_changed, sizeof(unsigned long long) * total, cudaMemcpyDeviceToHost, s));
     GLP_BCUDA(cudaStreamSynchronize(s));
-    for (int32_t i = 0; i < niter; ++i) changed[i] = (int64_t)tmp[i];
+    for (int32_t i = 0; i < total; ++i) changed[i] = (int64_t)tmp[i];
   }
   return check_batch_err(b, s);
 }

@@ -21,6 +21,7 @@
 
 #include "engine.h"
 #include "hooks_engine.cuh"
+#include "smem_attr.h"
 
 namespace glp {
 
@@ -138,6 +139,9 @@ static void free_plan(DevicePlan* p) {
   *p = DevicePlan{};
 }
 
+// Plan set-up copies and clears go on the handle's stream (a pageable
+// source is staged before the call returns); ensure_plan synchronises that
+// stream before any step kernel, on whatever stream, can read the plan.
 template <class T>
 static int upload(DevicePlan* p, const std::vector<T>& v, T** out) {
   *out = nullptr;
@@ -145,7 +149,7 @@ static int upload(DevicePlan* p, const std::vector<T>& v, T** out) {
   void* d = nullptr;
   GLP_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
   p->allocs.push_back(d);
-  GLP_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  GLP_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, p->setup));
   *out = static_cast<T*>(d);
   return GLP_OK;
 }
@@ -173,7 +177,7 @@ static int zeroed(DevicePlan* p, size_t count, T** out) {
   void* d = nullptr;
   GLP_CUDA(cudaMalloc(&d, count * sizeof(T)));
   p->allocs.push_back(d);
-  GLP_CUDA(cudaMemset(d, 0, count * sizeof(T)));
+  GLP_CUDA(cudaMemsetAsync(d, 0, count * sizeof(T), p->setup));
   *out = static_cast<T*>(d);
   return GLP_OK;
 }
@@ -190,6 +194,7 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   HostPlan hp;
   DevicePlan& p = g->plan;
   p.tiers = t;
+  p.setup = g->stream;
   int rc;
   int64_t n_mid = 0, n_big = 0, ntier[5] = {0, 0, 0, 0, 0};
   if (g->deg_sorted == 1) {
@@ -282,6 +287,11 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
       return GLP_ENOTSUP;
     }
   }
+  const cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) {
+    free_plan(&p);
+    return cuda_fail(e, "plan upload");
+  }
   p.valid = true;
   return GLP_OK;
 }
@@ -289,8 +299,8 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
 // --------------------------------------------------------------- launches
 template <class K>
 static int allow_smem(K kernel, size_t bytes) {
-  // static + dynamic shared memory above 48 KB needs the opt-in; set it always
-  GLP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  // static + dynamic shared memory above 48 KB needs the opt-in
+  GLP_CUDA(raise_smem_limit((const void*)kernel, bytes));
   return GLP_OK;
 }
 
@@ -568,7 +578,8 @@ static int ensure_work(glp_graph* g, int32_t total_iters) {
   }
   if (!g->d_err) {
     GLP_CUDA(cudaMalloc(&g->d_err, sizeof(uint32_t)));
-    GLP_CUDA(cudaMemset(g->d_err, 0, sizeof(uint32_t)));
+    GLP_CUDA(cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), g->stream));
+    GLP_CUDA(cudaStreamSynchronize(g->stream));
   }
   if (g->changed_cap < total_iters + 1) {
     if (g->d_changed) cudaFree(g->d_changed);

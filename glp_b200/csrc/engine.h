@@ -55,6 +55,7 @@ struct HostPlan {
 void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPlan* hp);
 
 struct DevicePlan {
+  cudaStream_t setup = nullptr;  // stream of the set-up copies (the handle's)
   TierParams tiers;
   bool valid = false;
   Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{}, big_lo{}, big_hi{};

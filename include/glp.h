@@ -204,11 +204,25 @@ void glp_free_host(void* p);
 typedef struct glp_batch glp_batch;
 int glp_batch_create(int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols, const int32_t* n,
                      const int64_t* m, int32_t on_device, glp_batch** out);
+/* As glp_batch_create, with a per-graph iteration count niter[g] (>= 0,
+ * non-decreasing over g, at most 8 distinct values) that glp_batch_run uses
+ * when given GLP_BATCH_OWN_ITERATIONS: graphs of smaller counts stop
+ * updating after their count; their labels are what a solo run of that
+ * count gives. */
+#define GLP_BATCH_OWN_ITERATIONS (-1)
+int glp_batch_create_ex(int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols, const int32_t* n,
+                        const int64_t* m, int32_t on_device, const int32_t* niter, glp_batch** out);
+/* Packs a new set of graphs into an existing batch, reusing its device
+ * buffers (they only grow): a round-by-round caller allocates nothing once
+ * the batch has seen its largest round.  Arguments as glp_batch_create_ex. */
+int glp_batch_repack(glp_batch* b, int32_t ngraphs, const int32_t* const* offsets, const int32_t* const* cols,
+                     const int32_t* n, const int64_t* m, int32_t on_device, const int32_t* niter);
 void glp_batch_destroy(glp_batch* b);
 int glp_batch_info(const glp_batch* b, int64_t* n, int64_t* m, int32_t* max_degree, int32_t* ngraphs);
-/* niter synchronous classic iterations of every graph.  labels: the packed
- * labels (host, or device when on_device); changed: optional host [niter]
- * labels changed per iteration over the batch.  params (nullable; other
+/* niter synchronous classic iterations of every graph (or, with
+ * GLP_BATCH_OWN_ITERATIONS, each graph's own count).  labels: the packed
+ * labels (host, or device when on_device); changed: optional host array of
+ * the largest iteration count, labels changed per iteration over the batch.  params (nullable; other
  * values = the tuned or default choice): tiny_max in {8,16,32} = largest
  * degree counted by one thread per vertex (above it, up to 32, lane groups);
  * mid_max 64 = degrees 33..64 by 16-lane groups, 32 = by whole warps;
@@ -225,6 +239,62 @@ int glp_batch_run(glp_batch* b, const glp_params* p, int32_t niter, int32_t* lab
  * the glp_batch_run parameter fields; times_ms (nullable, >= 12 entries)
  * the time of each candidate (-1: does not fit); ncand the candidate count. */
 int glp_batch_tune(glp_batch* b, int32_t probe_iters, glp_params* best, float* times_ms, int32_t* ncand);
+
+/* ----------------------------------------------------------------------
+ * Served LP.  No counterpart in the reference (it runs one graph per
+ * process).  A server keeps graphs and label state in HBM while requests of
+ * mixed size and method arrive: admission is FIFO against an HBM budget;
+ * small classic requests (unweighted, every degree <= 4096, at most
+ * batch_max_vertices vertices) are packed into rounds of the persistent
+ * batched kernel, each round taking every such request admitted so far
+ * (continuous batching at round granularity); the rest run as one-graph
+ * solves on plain_workers threads whose device work overlaps the rounds,
+ * shortest expected job first (aged by waiting time).
+ * Every result equals glp_run of that request alone. */
+typedef struct glp_server glp_server;
+typedef struct glp_server_config {
+  int32_t struct_size;         /* = sizeof(glp_server_config) */
+  int32_t device;              /* -1: the caller's current device */
+  int64_t hbm_budget_bytes;    /* admission budget (default 150e9) */
+  int32_t max_batch_graphs;    /* requests per batched round (default 4096) */
+  int32_t plain_workers;       /* concurrent one-graph solves (default 1) */
+  int32_t batch_max_vertices;  /* larger graphs take the one-graph path (default 2^22) */
+  int32_t reserved[8];
+} glp_server_config;
+typedef struct glp_request_stats {
+  double submit_s, admit_s, start_s, done_s; /* seconds since the server started */
+  int32_t path;                /* 0: one-graph engine, 1: batched round */
+  int32_t batch_graphs;        /* requests in its round (path 1) */
+  int32_t status;              /* GLP_OK or the failure code */
+  int32_t reserved[5];
+} glp_request_stats;
+int glp_server_config_default(glp_server_config* c);
+int glp_server_start(const glp_server_config* c, glp_server** out);
+/* Submits one solve of `method` for niter iterations on a HOST CSR; the
+ * labels land in labels_out (host, n entries).  offsets/cols/weights and
+ * labels_out must stay valid until the request is done.  *id names it. */
+int glp_server_submit(glp_server* s, const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n,
+                      int64_t m, int32_t method, const glp_params* p, int32_t niter, int32_t* labels_out,
+                      int64_t* id);
+/* Resident graphs: glp_server_add_graph copies a CSR (host, or device when
+ * on_device) into HBM once, counted against the budget; requests on it are
+ * submitted with glp_server_submit_graph and reuse it (and the plans built
+ * for it) with no upload; glp_server_remove_graph frees it once no request
+ * uses it. */
+int glp_server_add_graph(glp_server* s, const int32_t* offsets, const int32_t* cols, const int32_t* weights, int32_t n,
+                         int64_t m, int32_t on_device, int64_t* graph_id);
+int glp_server_submit_graph(glp_server* s, int64_t graph_id, int32_t method, const glp_params* p, int32_t niter,
+                            int32_t* labels_out, int64_t* id);
+int glp_server_remove_graph(glp_server* s, int64_t graph_id);
+/* GLP_EAGAIN while the request waits or runs; its status once done. */
+int glp_server_poll(glp_server* s, int64_t id, glp_request_stats* stats);
+/* Waits up to timeout_ms (< 0: no limit); GLP_ETIMEOUT when it runs out. */
+int glp_server_wait(glp_server* s, int64_t id, int32_t timeout_ms, glp_request_stats* stats);
+/* Forgets a finished request. */
+int glp_server_release(glp_server* s, int64_t id);
+int glp_server_info(glp_server* s, int64_t* pending, int64_t* in_flight, int64_t* used_bytes, int64_t* rounds);
+/* Finishes every submitted request, then stops the threads and frees. */
+int glp_server_stop(glp_server* s);
 
 /* ----------------------------------------------------------------------
  * Allocation-free classic LP.  No counterpart in the reference.

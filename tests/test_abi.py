@@ -49,6 +49,14 @@ def test_no_gpu_fails_loudly():
     with pytest.raises(_lib.GlpError) as e:
         Graph(g)
     assert e.value.code == _lib.GLP_ENODEV
+    from glp_b200.batch import Batch
+    from glp_b200.server import Server
+    with pytest.raises(_lib.GlpError) as e:
+        Batch([g])
+    assert e.value.code == _lib.GLP_ENODEV
+    with pytest.raises(_lib.GlpError) as e:
+        Server()
+    assert e.value.code == _lib.GLP_ENODEV
 
 
 def _plan(off, **kw):

@@ -140,3 +140,48 @@ def test_batch_workload_sample():
     with Batch(gs) as b:
         labels, changed = b.run(20)
         _check(b, gs, 20, labels, changed)
+
+
+def test_batch_per_graph_iteration_counts():
+    gs = _mixed()
+    niters = [3, 10, 0, 20, 10, 7, 1]
+    with Batch(gs, niters=niters) as b:
+        labels, changed = b.run(None)
+        assert len(changed) == 20
+        ch_sum = np.zeros(20, dtype=np.int64)
+        for g, k, lab in zip(gs, niters, b.split(labels)):
+            ref, ch = _solo(g, k)
+            np.testing.assert_array_equal(np.asarray(lab), ref, err_msg=f"niter {k}")
+            ch_sum[:k] += ch
+        np.testing.assert_array_equal(changed, ch_sum)
+        # a uniform count still applies to every graph
+        lab5, _ = b.run(5)
+        for g, lab in zip(gs, b.split(lab5)):
+            np.testing.assert_array_equal(np.asarray(lab), _solo(g, 5)[0])
+        # graph replay with per-graph counts and device labels
+        out = torch.empty(b.n, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            b.run(None, make_params(use_graph=1), labels_out=out)
+            np.testing.assert_array_equal(out.cpu().numpy(), labels)
+
+
+def test_batch_repack_reuses_the_object():
+    import ctypes as C
+    gs = _mixed()
+    with Batch(gs[:3]) as b:
+        lib = _lib.load()
+        for subset, k in ((gs[3:], 6), (gs[:5], 9), (gs, 4)):
+            G = len(subset)
+            offs = (C.c_void_p * G)(*[g.offsets.data_ptr() for g in subset])
+            cols = (C.c_void_p * G)(*[g.cols.data_ptr() if g.m else 0 for g in subset])
+            ns = np.array([g.n for g in subset], np.int32)
+            ms = np.array([g.m for g in subset], np.int64)
+            _lib.check(lib.glp_batch_repack(b._h, G, offs, cols, C.c_void_p(ns.ctypes.data),
+                                            C.c_void_p(ms.ctypes.data), 1, None))
+            n = int(ns.sum())
+            lab = np.empty(max(n, 1), np.int32)
+            _lib.check(lib.glp_batch_run(b._h, None, k, C.c_void_p(lab.ctypes.data), 0, None, None))
+            base = 0
+            for g in subset:
+                np.testing.assert_array_equal(lab[base:base + g.n], _solo(g, k)[0])
+                base += g.n
