@@ -51,7 +51,7 @@ TIER_PLAN_KEYS = {0: "tiny", 1: "group16", 2: "group32", 3: "mid", 4: "big", 5: 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="glp", choices=["glp", "reference"])
     ap.add_argument("--scale", type=int, default=24)
@@ -131,7 +131,7 @@ class ClockSampler:
             ident = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
         except Exception:
             ident = str(device)
-        self.cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+        self.cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
                     "-i", ident]
 
     def start(self):

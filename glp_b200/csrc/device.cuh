@@ -114,16 +114,18 @@ struct CountTable {
 };
 
 // Bounded insert: gives up after `max_probe` probes and returns kNoSlot.
-// Double hashing (odd stride from a second hash) avoids the long clustered
-// runs of linear probing, so the lanes of a warp finish their probes close
-// together.  Optionally appends newly claimed slots to `claimed`.
+// The home slot is the top bits of a Fibonacci (multiplicative) hash, one
+// multiply-high; on a collision the probe continues by double hashing with an
+// odd stride from other bits of the same product, so the lanes of a warp
+// finish their probes close together and the table can be half full.
+// Optionally appends newly claimed slots to `claimed`.
 constexpr uint32_t kNoSlot = 0xffffffffu;
 __device__ __forceinline__ uint32_t table_insert_bounded(uint32_t* keys, uint32_t* vals, uint32_t mask, uint32_t key,
                                                          uint32_t c, uint32_t max_probe, uint32_t* claimed,
                                                          uint32_t* nclaimed) {
-  const uint32_t hk = fmix32(key);
-  uint32_t h = hk & mask;
-  const uint32_t step = (fmix32(hk ^ 0x5bd1e995u) | 1u) & mask;
+  const uint32_t hk = key * 0x9E3779B1u;
+  uint32_t h = __umulhi(hk, mask + 1u);
+  uint32_t step = 0;
   for (uint32_t probe = 0; probe < max_probe; ++probe) {
     const uint32_t cur = keys[h];
     if (cur == key) return atomicAdd(&vals[h], c) + c;
@@ -135,9 +137,20 @@ __device__ __forceinline__ uint32_t table_insert_bounded(uint32_t* keys, uint32_
       }
       if (prev == key) return atomicAdd(&vals[h], c) + c;
     }
-    h = (h + (step ? step : 1u)) & mask;
+    if (step == 0) {
+      step = ((hk >> 9) | 1u) & mask;
+      if (step == 0) step = 1u;
+    }
+    h = (h + step) & mask;
   }
   return kNoSlot;
+}
+
+// Zeroes n words of shared memory with 16-byte stores (p 16-byte aligned, n a
+// multiple of 4); threads t, t+stride, ... of the caller's group take part.
+__device__ __forceinline__ void zero_words16(uint32_t* p, uint32_t n, uint32_t t, uint32_t stride) {
+  uint4* q = reinterpret_cast<uint4*>(p);
+  for (uint32_t s = t; s < n / 4; s += stride) q[s] = make_uint4(0u, 0u, 0u, 0u);
 }
 
 // Smallest power of two >= x (x >= 1).

@@ -1003,7 +1003,7 @@ __global__ void __launch_bounds__(NT) k_noalloc_step(const int32_t* __restrict__
                                                       const int32_t* __restrict__ cols,
                                                       const int32_t* __restrict__ lin, int32_t* __restrict__ lout,
                                                       int32_t n, unsigned long long* changed, uint32_t* err) {
-  extern __shared__ __align__(8) uint32_t smem[];
+  extern __shared__ __align__(16) uint32_t smem[];
   __shared__ Best red[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const ScoreClassic score;

@@ -169,7 +169,7 @@ __device__ __forceinline__ unsigned long long pack_best(const Best& b, uint32_t*
 
 // ---------------------------------------------------------------- tiny tier
 template <int TMAX, bool W, class S>
-__global__ void __launch_bounds__(256) k_tiny(StepArgs a, TierWork tw, S score) {
+__global__ void __launch_bounds__(256, TMAX >= 32 ? 2 : 1) k_tiny(StepArgs a, TierWork tw, S score) {
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
   // grid-stride over whole warps so record_changes sees full warps
@@ -360,8 +360,8 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
 template <int CAP, int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
-  __shared__ uint32_t skeys[NW][CAP];
-  __shared__ uint32_t svals[NW][CAP];
+  __shared__ __align__(16) uint32_t skeys[NW][CAP];
+  __shared__ __align__(16) uint32_t svals[NW][CAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
@@ -370,11 +370,9 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
   for (int32_t i = blockIdx.x * NW + warp; i < nwork; i += gridDim.x * NW) {
     const int32_t v = tw.at(mode, i);
     const int32_t b = a.off[v], e = a.off[v + 1];
-    const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));
-    for (uint32_t s = lane; s < cap; s += 32) {
-      kk[s] = 0;
-      vv[s] = 0;
-    }
+    const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));  // degree > 32: cap >= 128
+    zero_words16(kk, cap, lane, 32);
+    zero_words16(vv, cap, lane, 32);
     __syncwarp();
     Best best = best_none();
     bool fail = false;
@@ -412,7 +410,7 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
 // (dynamic, CAP slots) sized per vertex to the power of two >= 2*degree.
 template <int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
-  extern __shared__ __align__(8) uint32_t smem[];
+  extern __shared__ __align__(16) uint32_t smem[];
   __shared__ Best red[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
@@ -423,7 +421,7 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
     const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));
     uint32_t* keys = smem;
     uint32_t* vals = smem + cap;
-    for (uint32_t s = threadIdx.x; s < 2 * cap; s += NT) smem[s] = 0;
+    zero_words16(smem, 2 * cap, threadIdx.x, NT);  // degree > 32: cap >= 128
     __syncthreads();
     Best best = best_none();
     bool fail = false;
@@ -658,7 +656,7 @@ constexpr uint32_t kHubProbe = 64;
 
 template <int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_hub_bucket(StepArgs a, HubPlan hp, S score) {
-  extern __shared__ uint32_t hsm[];
+  extern __shared__ __align__(16) uint32_t hsm[];
   __shared__ Best red[32];
   __shared__ int overflow;
   for (int32_t it = blockIdx.x; it < hp.nitems; it += gridDim.x) {
@@ -676,7 +674,7 @@ __global__ void __launch_bounds__(NT) k_hub_bucket(StepArgs a, HubPlan hp, S sco
       for (uint32_t sub = 0; sub < nsub; ++sub) {
         uint32_t* keys = hsm;
         uint32_t* vals = hsm + cap;
-        for (uint32_t s = threadIdx.x; s < 2 * cap; s += NT) hsm[s] = 0;
+        zero_words16(hsm, 2 * cap, threadIdx.x, NT);  // cap >= 2
         __syncthreads();
         bool fail = false;
         auto ins = [&](uint32_t key, uint32_t k) {
