@@ -65,6 +65,7 @@ def parse():
                          "batched: the batched workload alone")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-suite", action="store_true", help="skip the layered / weighted / SLPA measurements")
     ap.add_argument("--requests", type=int, default=300, help="served workload: requests per arrival rate")
     ap.add_argument("--rates", default="50,200", help="served workload: Poisson arrival rates (req/s)")
     ap.add_argument("--serve-seed", type=int, default=6)
@@ -402,8 +403,74 @@ def run_glp(args, ws, rank, local):
         sv = run_served(args, ws, rank, local)
         if rank == 0:
             line["served"] = sv
+    if not args.no_suite:
+        su = run_suite(args, ws, rank, local)
+        if rank == 0:
+            line["suite"] = su
     if rank == 0:
         print(json.dumps(line))
+
+
+# ----------------------------------------------------------------- suite
+def run_suite(args, ws, rank, local):
+    """The other paths at scale, device time per run with the graph resident:
+    layered LP (5 layers x 10 iterations, gamma 1..1/16 -> dstar 2,3,5,9,17)
+    and classic LP, unweighted and with integer weights in [1, 16], on R-MAT
+    scale 24 (seed 2) and on a planted partition of 10M vertices in 1,000
+    communities (mean intra-degree 18, inter-degree 2, seed 3); SLPA (T = 20,
+    r = 0.1, 20 iterations) on the overlapping planted graph of 2M vertices
+    (2,000 communities, overlap 0.1, mean degree 24, seed 4).  Roofline bytes
+    per iteration: classic 8m+12n+4, weighted +4m, layered 8m+16n+4 (+4m
+    weighted), SLPA step 8m+16n+4."""
+    from glp_b200 import _lib, graphs
+    from glp_b200.engine import Graph, make_params
+
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    peak, peak_kind = measured_peak()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    out = []
+
+    def measure(name, g, method, niter, params, per_iter_bytes, iters_per_run):
+        n, m = g.n, g.m
+        with Graph(g) as h:
+            lab = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+            h.run(method, niter, params, labels_out=lab, stream=sp)  # warm-up
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 2
+            e0.record(stream)
+            for _ in range(reps):
+                h.run(method, niter, params, labels_out=lab, stream=sp)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1) / reps
+        it_ms = ms / iters_per_run
+        gbs = per_iter_bytes / (it_ms / 1e3) / 1e9
+        out.append({"workload": name, "n": n, "m": m, "ms_per_run": round(ms, 3), "iterations": iters_per_run,
+                    "gteps_per_iter": round(m / (it_ms / 1e3) / 1e9, 2), "achieved_gbs": round(gbs, 1),
+                    "frac": round(gbs / peak, 4), "bytes_per_iter": int(per_iter_bytes)})
+
+    gammas = make_params(dstar=[2, 3, 5, 9, 17])
+    for gname, builder in (("rmat24-seed2", lambda w: graphs.rmat(24, 16, seed=2, device=dev, weighted=w)),
+                           ("planted10M-k1000-seed3",
+                            lambda w: graphs.planted(10_000_000, 1000, 18.0, 2.0, seed=3, device=dev, weighted=w))):
+        for weighted in (False, True):
+            g = builder(weighted)
+            n, m = g.n, g.m
+            wb = 4 * m if weighted else 0
+            tag = f"{gname}{'-weighted' if weighted else ''}"
+            measure(f"classic-{tag}-20it", g, _lib.METHOD_CLASSIC, 20, None, 8 * m + 12 * n + 4 + wb, 20)
+            measure(f"layered-{tag}-5x10it", g, _lib.METHOD_LAYERED, 10, gammas, 8 * m + 16 * n + 4 + wb, 50)
+            del g
+            torch.cuda.empty_cache()
+    g = graphs.overlapping(2_000_000, 2000, 0.1, 24.0, seed=4, device=dev)
+    measure("slpa-overlap2M-k2000-seed4-T20", g, _lib.METHOD_SLPA, 20,
+            make_params(slpa_T=20, slpa_r=0.1, seed=4), 8 * g.m + 16 * g.n + 4, 20)
+    del g
+    torch.cuda.empty_cache()
+    return {"peak_gbs": peak, "peak_kind": peak_kind, "runs": out,
+            "how": "device time (CUDA events) of 2 runs after 1 warm-up run, graph resident, labels on the device"}
 
 
 # ----------------------------------------------------------------- served

@@ -72,6 +72,38 @@ __device__ __forceinline__ void record_change(const StepArgs& a, int32_t v) {
   if (a.chg_out) a.chg_out[atomicAdd(a.chg_out_n, 1u)] = v;
 }
 
+// Batched recording for kernels that decide one vertex per warp: lane 0
+// keeps the warp's changed vertices in a 32-entry shared buffer, and a full
+// (or final) buffer costs one add to the counter and one reservation in the
+// list, written by the whole warp.  Almost every vertex changes in the first
+// steps, and a per-vertex atomic on the two shared counters would serialise
+// there.
+__device__ __forceinline__ void warp_flush_changes(const StepArgs& a, const int32_t* buf, uint32_t nb) {
+  if (!nb) return;
+  const int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (lane == 0) {
+    atomicAdd(a.changed, (unsigned long long)nb);
+    if (a.chg_out) base = atomicAdd(a.chg_out_n, nb);
+  }
+  if (a.chg_out) {
+    base = __shfl_sync(kFull, base, 0);
+    __syncwarp();
+    if ((uint32_t)lane < nb) a.chg_out[base + lane] = buf[lane];
+  }
+  __syncwarp();
+}
+// Called by every lane after each vertex; `changed` and v matter on lane 0.
+__device__ __forceinline__ void warp_note_change(const StepArgs& a, int32_t* buf, uint32_t& nb, bool changed,
+                                                 int32_t v) {
+  if ((threadIdx.x & 31) == 0 && changed) buf[nb] = v;
+  nb += __shfl_sync(kFull, changed ? 1u : 0u, 0);
+  if (nb == 32) {
+    warp_flush_changes(a, buf, nb);
+    nb = 0;
+  }
+}
+
 // Step modes.  Full: every vertex counts exactly.  Majority: a streaming
 // pre-pass decides vertices whose own label holds a strict majority and
 // lists the others.  Frontier: only vertices with a neighbour that changed in
@@ -362,6 +394,8 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
   __shared__ __align__(16) uint32_t skeys[NW][CAP];
   __shared__ __align__(16) uint32_t svals[NW][CAP];
+  __shared__ int32_t cbuf[NW][32];  // changed vertices not yet listed
+  uint32_t ncb = 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
@@ -397,12 +431,27 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
     }
     if (fail) atomicOr(a.err, kErrProbe);
     best = group_max<32>(best);
+    bool chg = false;
     if (lane == 0) {
       a.lout[v] = best.l;
-      if (best.l != a.lcur[v]) record_change(a, v);
+      chg = best.l != a.lcur[v];
     }
-    __syncwarp();
+    warp_note_change(a, cbuf[warp], ncb, chg, v);
+    __syncwarp();  // the table is cleared for the next vertex
   }
+  warp_flush_changes(a, cbuf[warp], ncb);
+}
+
+// One thread's batch of changed vertices: one add to the counter and one
+// reservation in the list for the whole batch.
+__device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32_t* buf, uint32_t& nb) {
+  if (!nb) return;
+  atomicAdd(a.changed, (unsigned long long)nb);
+  if (a.chg_out) {
+    const uint32_t base = atomicAdd(a.chg_out_n, nb);
+    for (uint32_t i = 0; i < nb; ++i) a.chg_out[base + i] = buf[i];
+  }
+  nb = 0;
 }
 
 // ----------------------------------------------------------------- big tier
@@ -411,6 +460,8 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
 template <int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
   extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ int32_t cbuf[64];  // changed vertices not yet listed (thread 0's)
+  uint32_t ncb = 0;
   __shared__ Best red[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
@@ -448,9 +499,13 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0) {
       a.lout[v] = best.l;
-      if (best.l != a.lcur[v]) record_change(a, v);
+      if (best.l != a.lcur[v]) {
+        cbuf[ncb++] = v;
+        if (ncb == 64) flush_big_changes(a, cbuf, ncb);
+      }
     }
   }
+  if (threadIdx.x == 0) flush_big_changes(a, cbuf, ncb);
 }
 
 // ----------------------------------------------------------------- hub tier
