@@ -236,7 +236,7 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   ntier[3] = p.mid.n;
   ntier[4] = p.big.n;
   if ((rc = zeroed(&p, 9, &p.counts)) || (rc = zeroed(&p, std::max<size_t>((size_t)n_mid, 1), &p.fmid.ids)) ||
-      (rc = zeroed(&p, std::max<size_t>((size_t)n_big, 1), &p.fbig.ids)) || (rc = zeroed(&p, 1, &p.d_mode)) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)n_big, 1), &p.fbig.ids)) || (rc = zeroed(&p, 2, &p.d_mode)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.front.act)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[0])) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[1]))) {
@@ -331,7 +331,8 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   const bool modal = a.mode != nullptr;
   if (modal) {
     GLP_CUDA(cudaMemsetAsync(p.counts, 0, 7 * sizeof(uint32_t), s));
-    k_step_mode<<<1, 1, 0, s>>>(L.prev_changed, a.n, L.allow_majority, L.allow_frontier, p.d_mode);
+    k_step_mode<<<1, 1, 0, s>>>(L.prev_changed, a.n, a.n - (int32_t)p.isolated, L.allow_majority,
+                                L.allow_frontier, p.d_mode);
     ++*launches;
     if (L.allow_frontier && L.front.chg_in) {
       const unsigned fgrid = 148 * 16;
@@ -709,9 +710,15 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       }
       int32_t* lin = g->d_lab[it & 1];
       int32_t* lout = g->d_lab[(it + 1) & 1];
+      // full counting every step; the step mode only chooses how the volume
+      // term is looked up (from the previous step's changes within the layer)
       StepArgs a{g->d_off, g->d_cols, g->d_w, lin,     lin,   lout, g->d_changed + step, g->d_err,
-                 nullptr, g->n,   nullptr, nullptr};  // full counting every step
-      if ((rc = launch_step<W>(c.launch(), a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches))) return rc;
+                 g->plan.d_mode, g->n, nullptr, nullptr};
+      StepLaunch L = c.launch();
+      L.prev_changed = it > 0 ? g->d_changed + step - 1 : nullptr;
+      L.allow_majority = 0;
+      L.allow_frontier = 0;
+      if ((rc = launch_step<W>(L, a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches))) return rc;
       if ((rc = c.aux_mark(0))) return rc;
       k_histogram<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(lout, g->n, vol_w);
       ++c.launches;

@@ -115,16 +115,24 @@ __device__ __forceinline__ bool use_majority(const StepArgs& a) { return step_mo
 
 // Picks the mode from the previous step's changed count: frontier below n/20
 // changes (when allowed), majority below n/4 (when allowed), else full.
-__global__ void k_step_mode(const unsigned long long* prev_changed, int32_t n, int allow_majority,
+// mode[1] (scores that need a per-label lookup, layered LP): 1 = score each
+// distinct label once from the finished table, worth it once fewer than half
+// of the n_active non-isolated vertices changed (their neighbourhoods hold
+// few distinct labels); 0 = score at every insert, the lookup issued before
+// the insert so that its latency overlaps the hashing.
+__global__ void k_step_mode(const unsigned long long* prev_changed, int32_t n, int32_t n_active, int allow_majority,
                             int allow_frontier, int32_t* mode) {
-  int32_t m = kModeFull;
+  int32_t m = kModeFull, scan = 0;
   if (prev_changed) {
     const unsigned long long c = *prev_changed;
     if (allow_frontier && c * 20ull < (unsigned long long)n) m = kModeFrontier;
     else if (allow_majority && c * 4ull < (unsigned long long)n) m = kModeMajority;
+    scan = c * 2ull < (unsigned long long)n_active ? 1 : 0;
   }
-  *mode = m;
+  mode[0] = m;
+  mode[1] = scan;
 }
+__device__ __forceinline__ bool scan_scores(const StepArgs& a) { return a.mode && a.mode[1] != 0; }
 
 // The vertices of one tier: explicit ids, or the contiguous range
 // [base, base+n) (degree-sorted graphs make every tier contiguous).
@@ -167,18 +175,27 @@ struct TierWork {
 // majority shortcut applies.
 struct ScoreClassic {
   static constexpr bool kMajority = true;
+  static constexpr bool kScan = false;  // no lookup: running maximum at every insert
   __device__ __forceinline__ int64_t operator()(int32_t, uint32_t k) const { return (int64_t)k; }
+  __device__ __forceinline__ int32_t vol_of(int32_t) const { return 0; }
+  __device__ __forceinline__ int64_t from_vol(uint32_t k, int32_t) const { return (int64_t)k; }
 };
 
 // score(l, k) for layered LP: dstar*k - vol_r[l] (kernel.cuh:2575-2600).
 // The volume term breaks the majority argument: no shortcut.
 struct ScoreLayered {
   static constexpr bool kMajority = false;
+  // the volume is a global lookup per label: prefetched per insert, or (step
+  // mode word 1) looked up once per distinct label by a scan of the table
+  static constexpr bool kScan = true;
   const int32_t* vol;
   int64_t dstar;
   __device__ __forceinline__ int64_t operator()(int32_t l, uint32_t k) const {
     return dstar * (int64_t)k - (int64_t)__ldg(vol + l);
   }
+  // the same split in two, so that callers can issue the loads together
+  __device__ __forceinline__ int32_t vol_of(int32_t l) const { return __ldg(vol + l); }
+  __device__ __forceinline__ int64_t from_vol(uint32_t k, int32_t v) const { return dstar * (int64_t)k - (int64_t)v; }
 };
 
 template <bool W>
@@ -221,6 +238,11 @@ __global__ void __launch_bounds__(256, TMAX >= 32 ? 2 : 1) k_tiny(StepArgs a, Ti
       wt[i] = 0;
       if (i < d) load_edge<W>(a, (int64_t)b + i, lab[i], wt[i]);
     }
+    // every label's volume (layered LP) is loaded before the compares, so the
+    // loads are in flight together
+    int32_t vl[TMAX];
+#pragma unroll
+    for (int i = 0; i < TMAX; ++i) vl[i] = (S::kScan && i < d) ? score.vol_of(lab[i]) : 0;
     Best best = best_none();
 #pragma unroll
     for (int i = 0; i < TMAX; ++i) {
@@ -228,7 +250,7 @@ __global__ void __launch_bounds__(256, TMAX >= 32 ? 2 : 1) k_tiny(StepArgs a, Ti
         uint32_t k = 0;
 #pragma unroll
         for (int j = 0; j < TMAX; ++j) k += (lab[j] == lab[i]) ? wt[j] : 0u;
-        const Best c{score(lab[i], k), lab[i]};
+        const Best c{score.from_vol(k, vl[i]), lab[i]};
         if (better(c, best)) best = c;
       }
     }
@@ -307,7 +329,7 @@ __global__ void __launch_bounds__(256) k_group(StepArgs a, TierWork tw, S score)
 // lanes of the warp.
 template <bool W, class S, class Ins>
 __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, const S& score, const Ins& insert,
-                                            Best& best, bool& fail) {
+                                            Best& best, bool& fail, bool scan = false) {
   const int lane = threadIdx.x & 31;
   const int32_t l0 = __shfl_sync(kFull, has ? lab : -1, 0);
   const uint32_t m0 = __ballot_sync(kFull, has && lab == l0);
@@ -318,12 +340,40 @@ __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, 
     else if (has && lab == l0) has = false;  // counted by lane 0
   }
   if (!has) return;
+  const int32_t vl = (S::kScan && !scan) ? score.vol_of(lab) : 0;  // in flight during the insert
   const uint32_t tot = insert((uint32_t)lab + 1u, k);
   if (tot == kNoSlot) {
     fail = true;
-  } else {
-    const Best c{score(lab, tot), lab};
+  } else if (!scan) {
+    const Best c{score.from_vol(tot, vl), lab};
     if (better(c, best)) best = c;
+  }
+}
+
+// The best (score, label) over the occupied slots of a finished table, slots
+// t, t+stride, ... of it (scores with kScan).
+// Eight slots a round, their volume loads in flight together.
+template <class S>
+__device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t* vals, uint32_t cap, uint32_t t,
+                                           uint32_t stride, const S& score, Best& best) {
+  constexpr int U = 8;
+  for (uint32_t s0 = t; s0 < cap; s0 += U * stride) {
+    uint32_t key[U], val[U];
+    int32_t vl[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint32_t s = s0 + u * stride;
+      key[u] = s < cap ? keys[s] : 0u;
+      val[u] = s < cap ? vals[s] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) vl[u] = key[u] ? score.vol_of((int32_t)(key[u] - 1u)) : 0;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (key[u]) {
+        const Best c{score.from_vol(val[u], vl[u]), (int32_t)(key[u] - 1u)};
+        if (better(c, best)) best = c;
+      }
   }
 }
 
@@ -392,6 +442,7 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
 template <int CAP, int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
+  const bool scan = S::kScan && scan_scores(a);
   __shared__ __align__(16) uint32_t skeys[NW][CAP];
   __shared__ __align__(16) uint32_t svals[NW][CAP];
   __shared__ int32_t cbuf[NW][32];  // changed vertices not yet listed
@@ -427,9 +478,13 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
         if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + 32 * q < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail);
+        if (j0 + 32 * q < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
     }
     if (fail) atomicOr(a.err, kErrProbe);
+    if (scan) {
+      __syncwarp();
+      scan_table(kk, vv, cap, lane, 32, score, best);
+    }
     best = group_max<32>(best);
     bool chg = false;
     if (lane == 0) {
@@ -459,6 +514,7 @@ __device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32
 // (dynamic, CAP slots) sized per vertex to the power of two >= 2*degree.
 template <int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
+  const bool scan = S::kScan && scan_scores(a);
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ int32_t cbuf[64];  // changed vertices not yet listed (thread 0's)
   uint32_t ncb = 0;
@@ -493,9 +549,13 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
         if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + q * NT < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail);
+        if (j0 + q * NT < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
     }
     if (fail) atomicOr(a.err, kErrProbe);
+    if (scan) {  // block-uniform
+      __syncthreads();
+      scan_table(keys, vals, cap, threadIdx.x, NT, score, best);
+    }
     best = block_max<NT>(best, red);
     if (threadIdx.x == 0) {
       a.lout[v] = best.l;
@@ -711,6 +771,7 @@ constexpr uint32_t kHubProbe = 64;
 
 template <int NT, bool W, class S>
 __global__ void __launch_bounds__(NT) k_hub_bucket(StepArgs a, HubPlan hp, S score) {
+  const bool scan = S::kScan && scan_scores(a);
   extern __shared__ __align__(16) uint32_t hsm[];
   __shared__ Best red[32];
   __shared__ int overflow;
@@ -749,11 +810,15 @@ __global__ void __launch_bounds__(NT) k_hub_bucket(StepArgs a, HubPlan hp, S sco
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            if (k0 + q * NT < size) count_chunk<W>(l[q] >= 0, l[q], wt[q], score, ins, best, fail);
+            if (k0 + q * NT < size) count_chunk<W>(l[q] >= 0, l[q], wt[q], score, ins, best, fail, scan);
         }
         if (fail) overflow = 1;
         __syncthreads();
         if (overflow) break;  // block-uniform
+        if (scan) {  // block-uniform
+          scan_table(keys, vals, cap, threadIdx.x, NT, score, best);
+          __syncthreads();  // the next sub-pass clears the table
+        }
       }
       if (!overflow) break;
       if (nsub >= 1024u) {  // cannot happen for int32 sizes; stop rather than loop
