@@ -98,22 +98,27 @@ def barrier(ws):
         dist.barrier()
 
 
-def max_over_ranks(ws, x: float) -> float:
+def _reduce(ws, x: float, op) -> float:
     if ws == 1:
         return x
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    # NCCL reduces device tensors; the gloo backend (CPU tests) host ones
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(ws, x: float) -> float:
+    """The slowest rank's time: every multi-GPU figure is timed this way."""
+    import torch.distributed as dist
+    return _reduce(ws, x, dist.ReduceOp.MAX if ws > 1 else None)
 
 
 def sum_over_ranks(ws, x: float) -> float:
-    if ws == 1:
-        return x
+    """Work done by all ranks together (weak scaling: each rank a replica)."""
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(ws, x, dist.ReduceOp.SUM if ws > 1 else None)
 
 
 # ----------------------------------------------------------------- clocks
@@ -260,7 +265,7 @@ def run_reference(args, ws, rank):
         "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * t / len(timed), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the box",
-        "config": {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic", "n": n, "m": m,
+        "config": {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic-{args.iters}it", "n": n, "m": m,
                    "step": "one reference CPU iteration"},
         "impl": "reference",
         "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
