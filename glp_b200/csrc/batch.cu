@@ -299,26 +299,28 @@ __device__ __forceinline__ bool block_vertex(const BatchArgs& a, int32_t v, cons
   return threadIdx.x == 0 && best.l != lin[v];
 }
 
-// One vertex per thread (1 <= degree <= TT).
+// One vertex per thread (1 <= degree <= TT): its labels sorted in registers,
+// counts read off the runs (sort_labels).
 template <int TT>
 __device__ __forceinline__ bool thread_vertex(const BatchArgs& a, int32_t v, const int32_t* __restrict__ lin,
                                               int32_t* __restrict__ lout) {
   const int64_t b = a.off[v];
   const int32_t d = (int32_t)(a.off[v + 1] - b);
   int32_t lab[TT];
+  uint32_t one[TT];
 #pragma unroll
   for (int i = 0; i < TT; ++i) lab[i] = i < d ? ld_stream(a.cols + b + i) : -1;
 #pragma unroll
-  for (int i = 0; i < TT; ++i)
-    if (lab[i] >= 0) lab[i] = ld_label(lin + lab[i]);
+  for (int i = 0; i < TT; ++i) lab[i] = lab[i] >= 0 ? ld_label(lin + lab[i]) : INT32_MAX;
+  sort_labels<TT, false>(lab, one);
   Best best = best_none();
+  uint32_t run = 0;
 #pragma unroll
   for (int i = 0; i < TT; ++i) {
-    if (i < d) {
-      uint32_t k = 0;
-#pragma unroll
-      for (int j = 0; j < TT; ++j) k += lab[j] == lab[i] ? 1u : 0u;
-      const Best c{(int64_t)k, lab[i]};
+    run = (i > 0 && lab[i] == lab[i > 0 ? i - 1 : 0]) ? run + 1u : 1u;
+    const bool end = (i == TT - 1) || lab[(i + 1) & (TT - 1)] != lab[i];
+    if (end && lab[i] != INT32_MAX) {
+      const Best c{(int64_t)run, lab[i]};
       if (better(c, best)) best = c;
     }
   }

@@ -153,6 +153,40 @@ __device__ __forceinline__ void zero_words16(uint32_t* p, uint32_t n, uint32_t t
   for (uint32_t s = t; s < n / 4; s += stride) q[s] = make_uint4(0u, 0u, 0u, 0u);
 }
 
+// Sorts TMAX (a power of two) labels held in registers, ascending, with a
+// bitonic network (every index known at compile time, so nothing leaves the
+// registers); weights move with their labels when W.  Equal labels end up
+// adjacent, so a row's counts are the lengths (weight sums) of its runs:
+// O(TMAX log^2 TMAX) min/max steps instead of O(degree * TMAX) compares.
+template <int TMAX, bool W>
+__device__ __forceinline__ void sort_labels(int32_t (&lab)[TMAX], uint32_t (&wt)[TMAX]) {
+#pragma unroll
+  for (int k = 2; k <= TMAX; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < TMAX; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          const int32_t x = lab[i], y = lab[l];
+          if (W) {
+            const bool sw = up ? (x > y) : (x < y);
+            const uint32_t wx = wt[i], wy = wt[l];
+            lab[i] = sw ? y : x;
+            lab[l] = sw ? x : y;
+            wt[i] = sw ? wy : wx;
+            wt[l] = sw ? wx : wy;
+          } else {
+            lab[i] = up ? min(x, y) : max(x, y);
+            lab[l] = up ? max(x, y) : min(x, y);
+          }
+        }
+      }
+    }
+  }
+}
+
 // Smallest power of two >= x (x >= 1).
 __device__ __forceinline__ uint32_t pow2_ceil(uint32_t x) { return x <= 1 ? 1u : 1u << (32 - __clz(x - 1)); }
 

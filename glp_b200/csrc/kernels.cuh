@@ -218,7 +218,7 @@ __device__ __forceinline__ unsigned long long pack_best(const Best& b, uint32_t*
 
 // ---------------------------------------------------------------- tiny tier
 template <int TMAX, bool W, class S>
-__global__ void __launch_bounds__(256, TMAX >= 32 ? 2 : 1) k_tiny(StepArgs a, TierWork tw, S score) {
+__global__ void __launch_bounds__(256, (TMAX >= 32 && !W && !S::kScan) ? 2 : 1) k_tiny(StepArgs a, TierWork tw, S score) {
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
   // grid-stride over whole warps so record_changes sees full warps
@@ -234,23 +234,25 @@ __global__ void __launch_bounds__(256, TMAX >= 32 ? 2 : 1) k_tiny(StepArgs a, Ti
     uint32_t wt[TMAX];
 #pragma unroll
     for (int i = 0; i < TMAX; ++i) {
-      lab[i] = -1;
+      lab[i] = INT32_MAX;  // past the degree: sorts last, never scored
       wt[i] = 0;
       if (i < d) load_edge<W>(a, (int64_t)b + i, lab[i], wt[i]);
     }
-    // every label's volume (layered LP) is loaded before the compares, so the
+    sort_labels<TMAX, W>(lab, wt);
+    // every label's volume (layered LP) is loaded before the scan, so the
     // loads are in flight together
     int32_t vl[TMAX];
 #pragma unroll
-    for (int i = 0; i < TMAX; ++i) vl[i] = (S::kScan && i < d) ? score.vol_of(lab[i]) : 0;
+    for (int i = 0; i < TMAX; ++i) vl[i] = (S::kScan && lab[i] != INT32_MAX) ? score.vol_of(lab[i]) : 0;
+    // a run's total is scored at its last element
     Best best = best_none();
+    uint32_t run = 0;
 #pragma unroll
     for (int i = 0; i < TMAX; ++i) {
-      if (i < d) {
-        uint32_t k = 0;
-#pragma unroll
-        for (int j = 0; j < TMAX; ++j) k += (lab[j] == lab[i]) ? wt[j] : 0u;
-        const Best c{score.from_vol(k, vl[i]), lab[i]};
+      run = (i > 0 && lab[i] == lab[i > 0 ? i - 1 : 0]) ? run + wt[i] : wt[i];
+      const bool end = (i == TMAX - 1) || lab[(i + 1) & (TMAX - 1)] != lab[i];
+      if (end && lab[i] != INT32_MAX) {
+        const Best c{score.from_vol(run, vl[i]), lab[i]};
         if (better(c, best)) best = c;
       }
     }
