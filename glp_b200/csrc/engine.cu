@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 
 #include "engine.h"
@@ -40,6 +41,45 @@ void set_error(const char* fmt, ...) {
 int cuda_fail(cudaError_t e, const char* what) {
   set_error("%s: %s", what, cudaGetErrorString(e));
   return e == cudaErrorMemoryAllocation ? GLP_ENOMEM : GLP_ECUDA;
+}
+
+// Device memory of graph handles comes from the device's stream-ordered pool,
+// set once per device to keep freed memory in this process (release
+// threshold at its maximum): handles created and destroyed in a loop reuse
+// memory instead of mapping and unmapping gigabytes every time.  An
+// allocation is complete when dev_alloc returns (its stream is synchronised),
+// so any stream may use it; dev_free is called only once no stream uses the
+// memory any more.
+static std::once_flag g_pool_once[64];
+static cudaError_t dev_alloc_raw(void** p, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 64)
+    std::call_once(g_pool_once[dev], [dev] {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+    });
+  e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), cudaStreamPerThread);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+  return e;
+}
+template <class T>
+static cudaError_t dev_alloc(T** p, size_t bytes) {
+  return dev_alloc_raw(reinterpret_cast<void**>(p), bytes);
+}
+static void dev_free(void* p) {
+  if (p) cudaFreeAsync(p, cudaStreamPerThread);
+}
+
+// Waits for every stream a handle's work may be on.
+static int quiesce(glp_graph* g) {
+  for (cudaStream_t st : {g->stream, g->aux[0], g->aux[1], g->last_stream})
+    if (st) GLP_CUDA(cudaStreamSynchronize(st));
+  return GLP_OK;
 }
 
 static int require_device() {
@@ -135,7 +175,7 @@ void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPla
 }
 
 static void free_plan(DevicePlan* p) {
-  for (void* a : p->allocs) cudaFree(a);
+  for (void* a : p->allocs) dev_free(a);
   *p = DevicePlan{};
 }
 
@@ -147,7 +187,7 @@ static int upload(DevicePlan* p, const std::vector<T>& v, T** out) {
   *out = nullptr;
   if (v.empty()) return GLP_OK;
   void* d = nullptr;
-  GLP_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+  GLP_CUDA(dev_alloc(&d, v.size() * sizeof(T)));
   p->allocs.push_back(d);
   GLP_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, p->setup));
   *out = static_cast<T*>(d);
@@ -175,7 +215,7 @@ static int zeroed(DevicePlan* p, size_t count, T** out) {
   *out = nullptr;
   if (count == 0) return GLP_OK;
   void* d = nullptr;
-  GLP_CUDA(cudaMalloc(&d, count * sizeof(T)));
+  GLP_CUDA(dev_alloc(&d, count * sizeof(T)));
   p->allocs.push_back(d);
   GLP_CUDA(cudaMemsetAsync(d, 0, count * sizeof(T), p->setup));
   *out = static_cast<T*>(d);
@@ -565,27 +605,27 @@ static int after_iter(RunCtx& c, int32_t iter, const int32_t* d_labels) {
 
 static int grow(int32_t** p, int64_t* have, int64_t need) {
   if (*have >= need && *p) return GLP_OK;
-  if (*p) cudaFree(*p);
+  if (*p) dev_free(*p);
   *p = nullptr;
-  GLP_CUDA(cudaMalloc(p, std::max<int64_t>(need, 1) * sizeof(int32_t)));
+  GLP_CUDA(dev_alloc(p, std::max<int64_t>(need, 1) * sizeof(int32_t)));
   *have = need;
   return GLP_OK;
 }
 
 static int ensure_work(glp_graph* g, int32_t total_iters) {
   if (!g->d_lab[0]) {
-    GLP_CUDA(cudaMalloc(&g->d_lab[0], sizeof(int32_t) * std::max(g->n, 1)));
-    GLP_CUDA(cudaMalloc(&g->d_lab[1], sizeof(int32_t) * std::max(g->n, 1)));
+    GLP_CUDA(dev_alloc(&g->d_lab[0], sizeof(int32_t) * std::max(g->n, 1)));
+    GLP_CUDA(dev_alloc(&g->d_lab[1], sizeof(int32_t) * std::max(g->n, 1)));
   }
   if (!g->d_err) {
-    GLP_CUDA(cudaMalloc(&g->d_err, sizeof(uint32_t)));
+    GLP_CUDA(dev_alloc(&g->d_err, sizeof(uint32_t)));
     GLP_CUDA(cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), g->stream));
     GLP_CUDA(cudaStreamSynchronize(g->stream));
   }
   if (g->changed_cap < total_iters + 1) {
-    if (g->d_changed) cudaFree(g->d_changed);
+    if (g->d_changed) dev_free(g->d_changed);
     g->d_changed = nullptr;
-    GLP_CUDA(cudaMalloc(&g->d_changed, sizeof(unsigned long long) * (total_iters + 1)));
+    GLP_CUDA(dev_alloc(&g->d_changed, sizeof(unsigned long long) * (total_iters + 1)));
     g->changed_cap = total_iters + 1;
   }
   return GLP_OK;
@@ -608,13 +648,13 @@ static int ensure_sorted(glp_graph* g) {
     return GLP_OK;
   }
   uint32_t* d_bad = nullptr;
-  GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
+  GLP_CUDA(dev_alloc(&d_bad, sizeof(uint32_t)));
   GLP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), g->stream));
   k_check_sorted<<<148 * 32, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, d_bad);
   uint32_t bad = 1;
   GLP_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, g->stream));
   GLP_CUDA(cudaStreamSynchronize(g->stream));
-  cudaFree(d_bad);
+  dev_free(d_bad);
   g->rows_sorted = bad == 0 ? 1 : 0;
   return GLP_OK;
 }
@@ -640,13 +680,13 @@ static int ensure_symmetric(glp_graph* g) {
     return GLP_OK;
   }
   uint32_t* d_bad = nullptr;
-  GLP_CUDA(cudaMalloc(&d_bad, sizeof(uint32_t)));
+  GLP_CUDA(dev_alloc(&d_bad, sizeof(uint32_t)));
   GLP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), g->stream));
   k_check_symmetric<<<148 * 16, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, g->m, d_bad);
   uint32_t bad = 1;
   GLP_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, g->stream));
   GLP_CUDA(cudaStreamSynchronize(g->stream));
-  cudaFree(d_bad);
+  dev_free(d_bad);
   g->symmetric = bad == 0 ? 1 : 0;
   return GLP_OK;
 }
@@ -741,7 +781,7 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
   const int32_t T = p.slpa_T;
   int rc;
   if ((rc = grow(&g->d_mem, &g->mem_elems, (int64_t)T * g->n))) return rc;
-  if (!g->d_spoken) GLP_CUDA(cudaMalloc(&g->d_spoken, sizeof(int32_t) * std::max(g->n, 1)));
+  if (!g->d_spoken) GLP_CUDA(dev_alloc(&g->d_spoken, sizeof(int32_t) * std::max(g->n, 1)));
   GLP_CUDA(cudaMemsetAsync(g->d_mem, 0xff, sizeof(int32_t) * (size_t)T * g->n, c.s));
   if ((rc = init_labels(c))) return rc;
   for (int32_t it = 0; it < niter; ++it) {
@@ -775,8 +815,8 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
     int32_t* ncomm = out->slpa_ncomm;
     int32_t *tmp_c = nullptr, *tmp_n = nullptr;
     if (!dev) {
-      GLP_CUDA(cudaMalloc(&tmp_c, sizeof(int32_t) * (size_t)T * g->n));
-      GLP_CUDA(cudaMalloc(&tmp_n, sizeof(int32_t) * g->n));
+      GLP_CUDA(dev_alloc(&tmp_c, sizeof(int32_t) * (size_t)T * g->n));
+      GLP_CUDA(dev_alloc(&tmp_n, sizeof(int32_t) * g->n));
       comm = tmp_c;
       ncomm = tmp_n;
     }
@@ -788,8 +828,8 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
       if (out->slpa_ncomm)
         GLP_CUDA(cudaMemcpyAsync(out->slpa_ncomm, tmp_n, sizeof(int32_t) * g->n, cudaMemcpyDeviceToHost, c.s));
       GLP_CUDA(cudaStreamSynchronize(c.s));
-      cudaFree(tmp_c);
-      cudaFree(tmp_n);
+      dev_free(tmp_c);
+      dev_free(tmp_n);
     }
   }
   if (out->slpa_mem && g->n)
@@ -842,7 +882,7 @@ int validate_csr_device(glp_graph* g) {
     uint32_t unsorted;
   };
   Flags* d_f = nullptr;
-  GLP_CUDA(cudaMalloc(&d_f, sizeof(Flags)));
+  GLP_CUDA(dev_alloc(&d_f, sizeof(Flags)));
   GLP_CUDA(cudaMemset(d_f, 0, sizeof(Flags)));
   k_validate_offsets<<<1184, 256>>>(g->d_off, g->n, g->m, &d_f->bad, &d_f->maxdeg, &d_f->unsorted);
   Flags f{};
@@ -851,7 +891,7 @@ int validate_csr_device(glp_graph* g) {
     k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, &d_f->bad);
     e = cudaMemcpy(&f.bad, &d_f->bad, sizeof f.bad, cudaMemcpyDeviceToHost);
   }
-  cudaFree(d_f);
+  dev_free(d_f);
   if (e != cudaSuccess) return cuda_fail(e, "validate");
   if (f.bad & 16u) {
     set_error("offsets[0] must be 0 and offsets[n] must be m");
@@ -903,13 +943,13 @@ static int ensure_host_offsets(glp_graph* g) {
 
 static int device_bounds(glp_graph* g, const int32_t* thr, int k, int32_t* out) {
   int32_t* d = nullptr;
-  GLP_CUDA(cudaMalloc(&d, sizeof(int32_t) * 2 * k));
+  GLP_CUDA(dev_alloc(&d, sizeof(int32_t) * 2 * k));
   cudaError_t e = cudaMemcpy(d, thr, sizeof(int32_t) * k, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     k_tier_bounds<<<1, 32>>>(g->d_off, g->n, d, k, d + k);
     e = cudaMemcpy(out, d + k, sizeof(int32_t) * k, cudaMemcpyDeviceToHost);
   }
-  cudaFree(d);
+  dev_free(d);
   if (e != cudaSuccess) return cuda_fail(e, "tier bounds");
   return GLP_OK;
 }
@@ -943,8 +983,8 @@ static int hooks_iterations(RunCtx& c, H h, int32_t niter, int32_t step0, bool l
 static int run_hooks(RunCtx& c, const glp_params& p, int32_t niter) {
   glp_graph* g = c.g;
   if (g->max_degree > kHookSmemCap / 2 && !g->d_hook_keys) {
-    GLP_CUDA(cudaMalloc(&g->d_hook_keys, sizeof(uint32_t) * 2 * (size_t)g->m));
-    GLP_CUDA(cudaMalloc(&g->d_hook_vals, sizeof(double) * 2 * (size_t)g->m));
+    GLP_CUDA(dev_alloc(&g->d_hook_keys, sizeof(uint32_t) * 2 * (size_t)g->m));
+    GLP_CUDA(dev_alloc(&g->d_hook_vals, sizeof(double) * 2 * (size_t)g->m));
   }
   HookState st{g->d_off, g->d_cols, g->d_w, g->d_lab[0], g->d_lab[1], nullptr, nullptr, 1.0};
   c.iter_base = 1;  // Lnext holds the final labels
@@ -1113,14 +1153,14 @@ int glp_graph_create_ex(const int32_t* offsets, const int32_t* cols, const int32
   GLP_CUDA(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
   GLP_CUDA(cudaEventCreateWithFlags(&g->join[0], cudaEventDisableTiming));
   GLP_CUDA(cudaEventCreateWithFlags(&g->join[1], cudaEventDisableTiming));
-  GLP_CUDA(cudaMalloc(&g->d_off, sizeof(int32_t) * ((size_t)n + 1)));
+  GLP_CUDA(dev_alloc(&g->d_off, sizeof(int32_t) * ((size_t)n + 1)));
   GLP_CUDA(cudaMemcpy(g->d_off, offsets, sizeof(int32_t) * ((size_t)n + 1), kind));
   // 4 padding entries: tile kernels read columns as aligned 16-byte quads
-  GLP_CUDA(cudaMalloc(&g->d_cols, sizeof(int32_t) * (m + 4)));
+  GLP_CUDA(dev_alloc(&g->d_cols, sizeof(int32_t) * (m + 4)));
   GLP_CUDA(cudaMemset(g->d_cols + m, 0, sizeof(int32_t) * 4));
   if (m) GLP_CUDA(cudaMemcpy(g->d_cols, cols, sizeof(int32_t) * m, kind));
   if (weights) {
-    GLP_CUDA(cudaMalloc(&g->d_w, sizeof(int32_t) * (m + 4)));
+    GLP_CUDA(dev_alloc(&g->d_w, sizeof(int32_t) * (m + 4)));
     GLP_CUDA(cudaMemset(g->d_w + m, 0, sizeof(int32_t) * 4));
     if (m) GLP_CUDA(cudaMemcpy(g->d_w, weights, sizeof(int32_t) * m, kind));
   }
@@ -1133,20 +1173,21 @@ int glp_graph_create_ex(const int32_t* offsets, const int32_t* cols, const int32
 
 void glp_graph_destroy(glp_graph* g) {
   if (!g) return;
+  quiesce(g);  // no kernel of this handle may still use what is freed
   free_plan(&g->plan);
-  cudaFree(g->d_off);
-  cudaFree(g->d_cols);
-  cudaFree(g->d_w);
-  cudaFree(g->d_lab[0]);
-  cudaFree(g->d_lab[1]);
-  cudaFree(g->d_vol[0]);
-  cudaFree(g->d_vol[1]);
-  cudaFree(g->d_spoken);
-  cudaFree(g->d_mem);
-  cudaFree(g->d_changed);
-  cudaFree(g->d_err);
-  cudaFree(g->d_hook_keys);
-  cudaFree(g->d_hook_vals);
+  dev_free(g->d_off);
+  dev_free(g->d_cols);
+  dev_free(g->d_w);
+  dev_free(g->d_lab[0]);
+  dev_free(g->d_lab[1]);
+  dev_free(g->d_vol[0]);
+  dev_free(g->d_vol[1]);
+  dev_free(g->d_spoken);
+  dev_free(g->d_mem);
+  dev_free(g->d_changed);
+  dev_free(g->d_err);
+  dev_free(g->d_hook_keys);
+  dev_free(g->d_hook_vals);
   if (g->stream) cudaStreamDestroy(g->stream);
   for (cudaStream_t st : g->aux)
     if (st) cudaStreamDestroy(st);
@@ -1288,11 +1329,14 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
     return GLP_OK;
   }
   GLP_CUDA(cudaSetDevice(g->device));
+  if ((rc = quiesce(g))) return rc;  // set-up may free buffers an earlier async run still uses
   if ((rc = ensure_plan(g, t))) return rc;
   if ((rc = ensure_work(g, total))) return rc;
   RunCtx c;
   c.g = g;
   c.s = stream ? (cudaStream_t)stream : g->stream;
+  // a synchronous run has finished on return; an async one may still run on c.s
+  g->last_stream = p.async ? c.s : nullptr;
   c.cb = cb;
   c.user = cb_user;
   c.timing = out->tier_ms != nullptr;

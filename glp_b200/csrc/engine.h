@@ -120,6 +120,7 @@ struct glp_graph {
   int symmetric = -1;    // -1 unknown, 0 no, 1 yes (every edge stored both ways)
   int rows_sorted = -1;  // -1 unknown, 0 no, 1 every row strictly ascending
   int deg_sorted = 0;    // 1: degrees never increase along the vertex ids
+  cudaStream_t last_stream = nullptr;  // the stream of the latest run
   uint32_t epoch = 0;  // frontier mark of the last step
   // auxiliary streams and fork/join events of a step
   cudaStream_t aux[2] = {nullptr, nullptr};

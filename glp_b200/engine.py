@@ -167,14 +167,20 @@ class Graph:
             stream: int | None = None) -> Result:
         """Run `method` for `niter` iterations.  `callback(iter, labels_np)` sees
         the labels after every iteration (return True to stop).  With
-        `labels_out` (an int32 CUDA tensor of n) the labels stay on the device."""
+        `labels_out` (an int32 tensor of n) the labels land there: a CUDA
+        tensor keeps them on the device, a (pinned) CPU tensor receives them
+        without an intermediate copy."""
         p = params or _lib.default_params()
         total = niter * (p.nlayers if method == _lib.METHOD_LAYERED or
                          (method == _lib.METHOD_USER and p.hooks == _lib.HOOKS_LAYERED) else 1)
         out = _lib.Outputs()
-        on_dev = labels_out is not None
-        labels = labels_out if on_dev else np.empty(self.n, dtype=np.int32)
-        out.labels = labels.data_ptr() if on_dev else labels.ctypes.data
+        given = labels_out is not None
+        if given and (labels_out.dtype != torch.int32 or labels_out.numel() < self.n or
+                      not labels_out.is_contiguous()):
+            raise ValueError("labels_out must be a contiguous int32 tensor of n entries")
+        on_dev = given and labels_out.device.type == "cuda"
+        labels = labels_out if given else np.empty(self.n, dtype=np.int32)
+        out.labels = labels.data_ptr() if given else labels.ctypes.data
         out.on_device = 1 if on_dev else 0
         changed = np.zeros(max(total, 1), dtype=np.int64)
         if not p.async_:

@@ -86,7 +86,9 @@ typedef struct glp_params {
   int32_t async;                  /* 1: enqueue on the stream and return without
                                      synchronising (device outputs only, no
                                      callback); kernel error flags are then
-                                     reported by glp_graph_check() */
+                                     reported by glp_graph_check(); the
+                                     stream must stay valid until the next
+                                     call on the handle */
   int32_t reserved[8];
 } glp_params;
 

@@ -7,8 +7,9 @@ graphs drive every kernel (tiny, group16/32, mid, big, multi-chunk hub).
 """
 import numpy as np
 import pytest
+import torch
 
-from glp_b200 import _lib
+from glp_b200 import _lib, graphs
 from glp_b200.engine import Graph, make_params
 from glp_b200.graphs import from_numpy
 from oracle import oracle as O
@@ -281,3 +282,12 @@ def test_generators_host_equal_device():
     g2 = graphs.rmat(12, 16, seed=1, device="cuda", weighted=True)
     assert torch.equal(g1.offsets, g2.offsets.cpu()) and torch.equal(g1.cols, g2.cols.cpu())
     assert torch.equal(g1.weights, g2.weights.cpu())
+
+
+def test_labels_into_a_pinned_host_tensor():
+    g = graphs.rmat(12, 16, seed=1)
+    off, cols, _ = g.numpy()
+    out = torch.full((g.n,), -1, dtype=torch.int32).pin_memory()
+    with Graph(g) as h:
+        h.run(_lib.METHOD_CLASSIC, 7, labels_out=out)
+    np.testing.assert_array_equal(out.numpy(), O.classic_run(off, cols, 7))
