@@ -291,3 +291,50 @@ def test_labels_into_a_pinned_host_tensor():
     with Graph(g) as h:
         h.run(_lib.METHOD_CLASSIC, 7, labels_out=out)
     np.testing.assert_array_equal(out.numpy(), O.classic_run(off, cols, 7))
+
+
+def _oscillating_graph():
+    """Many small bipartite pieces (paths, even cycles, stars) that fall into a
+    period-2 oscillation under synchronous LP, next to an R-MAT part that
+    keeps changing for a while: the step modes switch while a third of the
+    vertices flip every step."""
+    edges, base = [], 0
+    rng = np.random.default_rng(5)
+    for k in range(400):
+        size = int(rng.integers(3, 9))
+        kind = k % 3
+        if kind == 0:    # path
+            edges += [(base + i, base + i + 1) for i in range(size - 1)]
+        elif kind == 1:  # even cycle
+            size += size % 2
+            edges += [(base + i, base + (i + 1) % size) for i in range(size)]
+        else:            # star
+            edges += [(base, base + i) for i in range(1, size)]
+        base += size
+    r = graphs.rmat(12, 8, seed=11)
+    ro, rc, _ = r.numpy()
+    for v in range(r.n):
+        for u in rc[ro[v]:ro[v + 1]]:
+            if v < u:
+                edges.append((base + v, base + int(u)))
+    return graphs.from_edges(base + r.n, edges, relabel=True)
+
+
+@pytest.mark.parametrize("niter", [3, 4, 40])
+def test_classic_oscillation_per_iteration(niter):
+    g = _oscillating_graph()
+    off, cols, _ = g.numpy()
+    _, otr = O.classic_run(off, cols, niter, trace=True)
+    prev = np.arange(g.n, dtype=np.int32)
+    ref_changed = []
+    for t in otr:
+        ref_changed.append(int((t != prev).sum()))
+        prev = t
+    with Graph(g) as h:  # symmetric CSR: frontier steps are allowed
+        trace = []
+        r = h.run(_lib.METHOD_CLASSIC, niter, callback=lambda it, lab: trace.append(lab) and False)
+        np.testing.assert_array_equal(np.array(trace), otr)
+        np.testing.assert_array_equal(r.changed, ref_changed)
+        r2 = h.run(_lib.METHOD_CLASSIC, niter)  # no per-iteration host sync
+        np.testing.assert_array_equal(r2.labels, otr[-1])
+        np.testing.assert_array_equal(r2.changed, ref_changed)
