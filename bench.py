@@ -250,19 +250,24 @@ def run_reference(args, ws, rank):
     n, m = len(off) - 1, len(cols)
     del g
     torch.cuda.empty_cache()
+    # a reference step is one CPU iteration of the full graph (about 30 s at
+    # scale 24 on 16 cores), so the run is bounded to 1 warm-up + 4 timed
+    # iterations whatever --steps / --warmup ask: the metric is per iteration
+    warm, steps = min(args.warmup, 1), max(1, min(args.steps, 4))
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "g.csr")
         write_csr(path, off, cols)
-        times = ref_cpulp_run(path, args.warmup + args.steps)
-    timed = times[args.warmup:]
+        times = ref_cpulp_run(path, warm + steps)
+    timed = times[warm:]
     t = sum(timed)
     value = m * len(timed) / t / 1e9
     cores = cpu_threads_used()
     sample = (f"CPUlp::sync_run_1 on the full R-MAT s{args.scale} graph (n={n}, m={m}); steps = reference LP "
-              f"iterations {args.warmup}..{args.warmup + args.steps - 1} after {args.warmup} warm-up iterations")
+              f"iterations {warm}..{warm + steps - 1} after {warm} warm-up iteration(s), bounded from "
+              f"--steps {args.steps} --warmup {args.warmup}")
     line = {
         "metric": f"classic LP GTEPS per iteration, R-MAT scale {args.scale}", "value": round(value, 4),
-        "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "unit": "GTEPS", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
         "ms_per_step": round(1000 * t / len(timed), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the box",
         "config": {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic-{args.iters}it", "n": n, "m": m,
