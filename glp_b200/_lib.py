@@ -94,6 +94,10 @@ SIGNATURES = {
     "glp_graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "glp_graph_plan": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(C.c_int64)]),
     "glp_graph_check": (C.c_int, [C.c_void_p]),
+    "glp_graph_cm_sketch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_void_p]),
+    "glp_graph_fa_summary": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,
+                                       C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "glp_plan_offsets": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Params), C.POINTER(C.c_int64)]),
     "glp_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Params), C.c_int32, C.POINTER(Outputs), ITER_CB,
                           C.c_void_p, C.c_void_p]),

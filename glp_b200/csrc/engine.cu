@@ -275,8 +275,9 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   ntier[2] = p.g32.n;
   ntier[3] = p.mid.n;
   ntier[4] = p.big.n;
-  if ((rc = zeroed(&p, 9, &p.counts)) || (rc = zeroed(&p, std::max<size_t>((size_t)n_mid, 1), &p.fmid.ids)) ||
+  if ((rc = zeroed(&p, 10, &p.counts)) || (rc = zeroed(&p, std::max<size_t>((size_t)n_mid, 1), &p.fmid.ids)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)n_big, 1), &p.fbig.ids)) || (rc = zeroed(&p, 2, &p.d_mode)) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)n_big, 1), &p.fscreen.ids)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.front.act)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[0])) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[1]))) {
@@ -286,6 +287,7 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   g->epoch = 0;  // fresh marks
   p.fmid.count = p.counts;
   p.fbig.count = p.counts + 1;
+  p.fscreen.count = p.counts + 9;
   p.front.tiny_max = t.tiny_max;
   p.front.mid_max = t.mid_max;
   p.front.big_max = t.big_max;
@@ -425,7 +427,27 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     if ((rc = mark_on(s, 7, 1))) return rc;
     ++*launches;
   }
-  if (p.big.n) {
+  if (p.big.n && L.backend != GLP_BACKEND_EXACT) {
+    // a summary screen decides what it can over the whole tier (its work
+    // lists included); the exact kernel takes the vertices it lists
+    const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
+    if ((rc = allow_smem(k_big<kBigNT, W, S>, sm))) return rc;
+    if ((rc = mark_on(s, 4, 0))) return rc;
+    GLP_CUDA(cudaMemsetAsync(p.fscreen.count, 0, sizeof(uint32_t), s));
+    TierWork all = work(p.big, 4, &p.fbig);
+    if (L.backend == GLP_BACKEND_CM) {
+      k_big_cm<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, 0, s>>>(a, all, score,
+                                                                                              p.fscreen);
+    } else {
+      constexpr int kFaNT = 128;
+      k_big_fa<kFaNT, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.big.n, kFaNT / 32), kMaxGrid), kFaNT, 0, s>>>(
+          a, all, score, p.fscreen);
+    }
+    TierWork rest{Verts{nullptr, 0, 0}, p.fscreen, FailList{nullptr, nullptr}, 0, 1};
+    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, rest, score);
+    *launches += 2;
+    if ((rc = mark_on(s, 4, 1))) return rc;
+  } else if (p.big.n) {
     // full mode: degrees <= kBigSplit in small-table blocks, the rest with the
     // full table; majority and frontier lists all go to the full-table launch
     const size_t sm_lo = 4ull * kBigSplit * sizeof(uint32_t);
@@ -506,6 +528,7 @@ struct RunCtx {
   std::vector<float> step_ms, step_tier;
   int64_t launches = 0;
   int iter_base = 0;
+  int32_t backend = GLP_BACKEND_EXACT;  // counting back-end of the big tier
 
   ~RunCtx() {
     for (auto& v : evs)
@@ -541,7 +564,9 @@ struct RunCtx {
       ran.back()[7] = p.mb.n > 0;
       ran.back()[8] = true;
     }
-    return StepLaunch{&g->plan, s, ev, {g->aux[0], g->aux[1]}, g->fork, {g->join[0], g->join[1]}};
+    StepLaunch L{&g->plan, s, ev, {g->aux[0], g->aux[1]}, g->fork, {g->join[0], g->join[1]}};
+    L.backend = backend;
+    return L;
   }
   cudaEvent_t* current() { return timing && used ? evs[used - 1].data() : nullptr; }
   int harvest() {
@@ -1255,6 +1280,104 @@ int glp_graph_check(glp_graph* g) {
   return check_err(g, g->stream);
 }
 
+// Device buffers of one summary inspection call, freed on every return path.
+struct InspectBufs {
+  std::vector<void*> held;
+  ~InspectBufs() {
+    for (void* p : held) dev_free(p);
+  }
+  int alloc(void** p, size_t bytes) {
+    GLP_CUDA(dev_alloc_raw(p, bytes));
+    held.push_back(*p);
+    return GLP_OK;
+  }
+};
+
+// Shared argument checks and uploads of glp_graph_cm_sketch / _fa_summary:
+// the labels (unless already on the device) and the vertex list.
+static int inspect_inputs(glp_graph* g, const int32_t* labels, int32_t on_device, const int32_t* vertices,
+                          int32_t nv, InspectBufs& bufs, const int32_t** d_lab, int32_t** d_verts) {
+  for (int32_t i = 0; i < nv; ++i)
+    if (vertices[i] < 0 || vertices[i] >= g->n) {
+      set_error("vertices[%d] = %d outside [0, %d)", i, vertices[i], g->n);
+      return GLP_EINVAL;
+    }
+  int rc = require_device();
+  if (rc) return rc;
+  GLP_CUDA(cudaSetDevice(g->device));
+  if ((rc = quiesce(g))) return rc;
+  if (on_device) {
+    *d_lab = labels;
+  } else {
+    int32_t* d = nullptr;
+    if ((rc = bufs.alloc((void**)&d, sizeof(int32_t) * (size_t)g->n))) return rc;
+    GLP_CUDA(cudaMemcpyAsync(d, labels, sizeof(int32_t) * (size_t)g->n, cudaMemcpyHostToDevice, g->stream));
+    *d_lab = d;
+  }
+  if ((rc = bufs.alloc((void**)d_verts, sizeof(int32_t) * (size_t)nv))) return rc;
+  GLP_CUDA(cudaMemcpyAsync(*d_verts, vertices, sizeof(int32_t) * (size_t)nv, cudaMemcpyHostToDevice, g->stream));
+  return GLP_OK;
+}
+
+int glp_graph_cm_sketch(glp_graph* g, const int32_t* labels, int32_t labels_on_device, const int32_t* vertices,
+                        int32_t nv, int32_t width, int32_t ref_compat, uint32_t* rows) {
+  if (!g || !labels || nv < 0 || (nv > 0 && (!vertices || !rows))) {
+    set_error("graph, labels, vertices and rows are required (nv=%d)", nv);
+    return GLP_EINVAL;
+  }
+  if (width < 1 || width > 4096) {
+    set_error("width %d outside [1, 4096]", width);
+    return GLP_EINVAL;
+  }
+  if (nv == 0 || g->n == 0) return GLP_OK;
+  InspectBufs bufs;
+  const int32_t* d_lab = nullptr;
+  int32_t* d_verts = nullptr;
+  uint32_t* d_rows = nullptr;
+  const size_t cells = 3ull * (size_t)width * (size_t)nv;
+  int rc = inspect_inputs(g, labels, labels_on_device, vertices, nv, bufs, &d_lab, &d_verts);
+  if (rc || (rc = bufs.alloc((void**)&d_rows, sizeof(uint32_t) * cells))) return rc;
+  k_cm_sketch<<<(unsigned)std::min<int32_t>(nv, 148 * 8), 256, 3u * (unsigned)width * sizeof(uint32_t), g->stream>>>(
+      g->d_off, g->d_cols, g->d_w, d_lab, d_verts, nv, width, ref_compat ? 1 : 0, d_rows);
+  GLP_CUDA(cudaGetLastError());
+  GLP_CUDA(cudaMemcpyAsync(rows, d_rows, sizeof(uint32_t) * cells, cudaMemcpyDeviceToHost, g->stream));
+  GLP_CUDA(cudaStreamSynchronize(g->stream));
+  return GLP_OK;
+}
+
+int glp_graph_fa_summary(glp_graph* g, const int32_t* labels, int32_t labels_on_device, const int32_t* vertices,
+                         int32_t nv, int32_t capacity, int32_t ref_compat, uint32_t* keys, uint32_t* vals,
+                         int32_t* rounds) {
+  if (!g || !labels || nv < 0 || (nv > 0 && (!vertices || !keys || !vals || !rounds))) {
+    set_error("graph, labels, vertices, keys, vals and rounds are required (nv=%d)", nv);
+    return GLP_EINVAL;
+  }
+  if (capacity < 1 || capacity > 65536) {
+    set_error("capacity %d outside [1, 65536]", capacity);
+    return GLP_EINVAL;
+  }
+  if (nv == 0 || g->n == 0) return GLP_OK;
+  InspectBufs bufs;
+  const int32_t* d_lab = nullptr;
+  int32_t* d_verts = nullptr;
+  uint32_t *d_keys = nullptr, *d_vals = nullptr;
+  int32_t* d_rounds = nullptr;
+  const size_t slots = (size_t)capacity * (size_t)nv;
+  int rc = inspect_inputs(g, labels, labels_on_device, vertices, nv, bufs, &d_lab, &d_verts);
+  if (rc || (rc = bufs.alloc((void**)&d_keys, sizeof(uint32_t) * slots)) ||
+      (rc = bufs.alloc((void**)&d_vals, sizeof(uint32_t) * slots)) ||
+      (rc = bufs.alloc((void**)&d_rounds, sizeof(int32_t) * (size_t)nv)))
+    return rc;
+  k_fa_summary<<<(unsigned)cdiv(nv, 128), 128, 0, g->stream>>>(g->d_off, g->d_cols, d_lab, d_verts, nv, capacity,
+                                                                 ref_compat ? 1 : 0, d_keys, d_vals, d_rounds);
+  GLP_CUDA(cudaGetLastError());
+  GLP_CUDA(cudaMemcpyAsync(keys, d_keys, sizeof(uint32_t) * slots, cudaMemcpyDeviceToHost, g->stream));
+  GLP_CUDA(cudaMemcpyAsync(vals, d_vals, sizeof(uint32_t) * slots, cudaMemcpyDeviceToHost, g->stream));
+  GLP_CUDA(cudaMemcpyAsync(rounds, d_rounds, sizeof(int32_t) * (size_t)nv, cudaMemcpyDeviceToHost, g->stream));
+  GLP_CUDA(cudaStreamSynchronize(g->stream));
+  return GLP_OK;
+}
+
 int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, glp_outputs* out, glp_iter_cb cb,
             void* cb_user, void* stream) {
   if (!g || !out || !out->labels) {
@@ -1339,6 +1462,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   g->last_stream = p.async ? c.s : nullptr;
   c.cb = cb;
   c.user = cb_user;
+  c.backend = p.backend;
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;

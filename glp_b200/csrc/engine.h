@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/glp.h"
+#include "backends.cuh"
 #include "kernels.cuh"
 
 namespace glp {
@@ -60,9 +61,10 @@ struct DevicePlan {
   bool valid = false;
   Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{}, big_lo{}, big_hi{};
   FailList fmid{}, fbig{};
+  FailList fscreen{};  // big-tier vertices a summary screen left to the exact kernel
   // list counters: [majority mid, majority big, frontier tiny, g16, g32, mid,
   // big] are zeroed at the start of every step; [7 + s] counts the changed
-  // list chg[s] that steps of parity s append to
+  // list chg[s] that steps of parity s append to; [9] counts fscreen
   uint32_t* counts = nullptr;
   int32_t* chg[2] = {nullptr, nullptr};
   Frontier front{};
@@ -87,6 +89,7 @@ struct StepLaunch {
   const unsigned long long* prev_changed = nullptr;
   int allow_majority = 0, allow_frontier = 0;
   Frontier front{};  // this step's frontier inputs (front.chg_in set from the second step)
+  int32_t backend = GLP_BACKEND_EXACT;  // GLP_BACKEND_CM / _FA: summary screen on the big tier
 };
 
 template <bool W, class S>

@@ -157,13 +157,16 @@ struct TierWork {
   FailList major;  // ids == nullptr: the tier has no pre-pass
   FailList front;
   int full_only;   // 1: works only in full mode (a sub-range of a tier)
+  int listed = 0;  // 1: works on the `major` list in every mode (screen fallbacks)
   __device__ __forceinline__ int32_t size(int32_t mode) const {
+    if (listed) return (int32_t)*major.count;
     if (full_only) return mode == kModeFull ? all.n : 0;
     if (mode == kModeFrontier && front.ids) return (int32_t)*front.count;
     if (mode == kModeMajority && major.ids) return (int32_t)*major.count;
     return all.n;
   }
   __device__ __forceinline__ int32_t at(int32_t mode, int64_t i) const {
+    if (listed) return major.ids[i];
     if (mode == kModeFrontier && front.ids) return front.ids[i];
     if (mode == kModeMajority && major.ids) return major.ids[i];
     return all[i];
@@ -179,6 +182,8 @@ struct ScoreClassic {
   __device__ __forceinline__ int64_t operator()(int32_t, uint32_t k) const { return (int64_t)k; }
   __device__ __forceinline__ int32_t vol_of(int32_t) const { return 0; }
   __device__ __forceinline__ int64_t from_vol(uint32_t k, int32_t) const { return (int64_t)k; }
+  // the largest score a label of count <= k can have
+  __device__ __forceinline__ int64_t bound(uint32_t k) const { return (int64_t)k; }
 };
 
 // score(l, k) for layered LP: dstar*k - vol_r[l] (kernel.cuh:2575-2600).
@@ -196,6 +201,8 @@ struct ScoreLayered {
   // the same split in two, so that callers can issue the loads together
   __device__ __forceinline__ int32_t vol_of(int32_t l) const { return __ldg(vol + l); }
   __device__ __forceinline__ int64_t from_vol(uint32_t k, int32_t v) const { return dstar * (int64_t)k - (int64_t)v; }
+  // the largest score a label of count <= k can have (volumes are >= 0)
+  __device__ __forceinline__ int64_t bound(uint32_t k) const { return dstar * (int64_t)k; }
 };
 
 template <bool W>

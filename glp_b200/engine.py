@@ -162,6 +162,37 @@ class Graph:
     def check(self) -> None:
         _lib.check(self._lib.glp_graph_check(self._h))
 
+    def _inspect_args(self, labels, vertices):
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        if lab.shape != (self.n,):
+            raise ValueError("labels must hold n int32 entries")
+        vs = np.ascontiguousarray(vertices, dtype=np.int32)
+        return lab, vs
+
+    def cm_sketch(self, labels, vertices, width: int, ref_compat: bool = False) -> np.ndarray:
+        """Count-min sketch (SharedCM<W,3>, method/countmin.cuh) of each listed
+        vertex's neighbourhood under `labels`, built on the device:
+        uint32 [len(vertices), 3, width]."""
+        lab, vs = self._inspect_args(labels, vertices)
+        rows = np.zeros((len(vs), 3, width), dtype=np.uint32)
+        _lib.check(self._lib.glp_graph_cm_sketch(self._h, lab.ctypes.data, 0, vs.ctypes.data, len(vs), width,
+                                                 int(ref_compat), rows.ctypes.data))
+        return rows
+
+    def fa_summary(self, labels, vertices, capacity: int, ref_compat: bool = False):
+        """Frequent-items table (SharedFA<C>, method/frequent.cuh) fed each listed
+        vertex's neighbour labels in CSR order, on the device: (keys, vals)
+        uint32 [len(vertices), capacity] (key = label+1, 0 = empty) and the
+        decrement rounds per vertex."""
+        lab, vs = self._inspect_args(labels, vertices)
+        keys = np.zeros((len(vs), capacity), dtype=np.uint32)
+        vals = np.zeros((len(vs), capacity), dtype=np.uint32)
+        rounds = np.zeros(len(vs), dtype=np.int32)
+        _lib.check(self._lib.glp_graph_fa_summary(self._h, lab.ctypes.data, 0, vs.ctypes.data, len(vs), capacity,
+                                                  int(ref_compat), keys.ctypes.data, vals.ctypes.data,
+                                                  rounds.ctypes.data))
+        return keys, vals, rounds
+
     def run(self, method: int, niter: int, params: _lib.Params | None = None, *, callback=None,
             labels_out: torch.Tensor | None = None, profile: bool = False, slpa_outputs: bool = False,
             stream: int | None = None) -> Result:

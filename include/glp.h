@@ -46,10 +46,15 @@ extern "C" {
 #define GLP_METHOD_SLPA 3    /* prop/SLPAprop.cuh, semantics tutorial/Base5prop.cuh */
 #define GLP_METHOD_USER 4    /* prop/UserdefinedLprop.cuh + README.md:72-101 hooks */
 
-/* ---- counting back-ends (method/hashtable.cuh, countmin.cuh, frequent.cuh) */
+/* ---- counting back-ends (method/hashtable.cuh, countmin.cuh, frequent.cuh)
+ * Every back-end gives the same labels, bit for bit.  CM and FA change how
+ * the big tier (degrees mid_max+1 .. big_max) counts: a summary decides the
+ * vertices whose mode it can prove, and the exact kernel counts the rest, as
+ * the reference's sketch kernel re-scans (header/kernel.cuh:1420-1566).  The
+ * other tiers always count exactly. */
 #define GLP_BACKEND_EXACT 0 /* shared/global hash tables (GlobalHT) */
-#define GLP_BACKEND_CM 1    /* count-min sketch screen + exact fallback */
-#define GLP_BACKEND_FA 2    /* Misra-Gries frequent table screen + exact fallback */
+#define GLP_BACKEND_CM 1    /* one-probe table + 3-row count-min sketch screen, exact fallback */
+#define GLP_BACKEND_FA 2    /* Misra-Gries frequent-items screen (one warp per vertex), exact fallback */
 
 /* ---- built-in hook sets for method 4 ----------------------------------- */
 #define GLP_HOOKS_CLASSIC 0 /* README.md:83-101 example: (L[sid], 1), score = freq */
@@ -149,6 +154,28 @@ int glp_graph_plan(glp_graph* g, const glp_params* p, int64_t out[16]);
 int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int64_t out[16]);
 /* Reports (and clears) kernel error flags raised by asynchronous runs. */
 int glp_graph_check(glp_graph* g);
+
+/* ---- counting summaries on the device (parity inspection) --------------
+ * The count-min sketch SharedCM<W,3> of method/countmin.cuh:9-262 built over
+ * the whole neighbourhood of each listed vertex under `labels` (n entries,
+ * host or device): every neighbour u adds its edge weight (1 when the graph
+ * is unweighted) to cell cm_hash_r(L[u]+1) % width of row r, with the row
+ * hashes of countmin.cuh:97-125.  ref_compat = 1 adds the third row's
+ * increment into the second row, as countmin.cuh:190 does.  rows: host,
+ * [nv][3][width] uint32; width in [1, 4096]. */
+int glp_graph_cm_sketch(glp_graph* g, const int32_t* labels, int32_t labels_on_device, const int32_t* vertices,
+                        int32_t nv, int32_t width, int32_t ref_compat, uint32_t* rows);
+/* The frequent-items table SharedFA<C> of method/frequent.cuh:10-106 fed the
+ * neighbour labels of each listed vertex one at a time in CSR order (edge
+ * weights are not used): key = label+1, linear probing from
+ * fmix32(key) % capacity, and when every slot holds another key a decrement
+ * round (clean: counts drop by one; ref_compat = 1: frequent.cuh:96-100 as
+ * written, every count becomes 0) after which the key is dropped; keys
+ * whose count was 1 are freed.  keys/vals: host [nv][capacity] (key 0 =
+ * empty slot); rounds: host [nv] decrement rounds.  capacity in [1, 65536]. */
+int glp_graph_fa_summary(glp_graph* g, const int32_t* labels, int32_t labels_on_device, const int32_t* vertices,
+                         int32_t nv, int32_t capacity, int32_t ref_compat, uint32_t* keys, uint32_t* vals,
+                         int32_t* rounds);
 
 /* Run `method` for niter iterations (layered: nlayers*niter).  Replaces
  * XProp<V,E>::run(niter) of prop/classicLprop.cuh:454-462,
