@@ -148,7 +148,7 @@ void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPla
     } else if (d <= t.big_max) {
       hp->big.push_back(v);
       hp->mb.push_back(v);
-      (d <= kBigSplit ? hp->big_lo : hp->big_hi).push_back(v);
+      (d <= kBigSplit ? hp->big_lo : d <= kBigTopSplit ? hp->big_hi : hp->big_top).push_back(v);
       tier = 5;
     } else {
       tier = 6;
@@ -240,22 +240,25 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   if (g->deg_sorted == 1) {
     // every tier is a contiguous range: its bounds come from binary searches
     // over the non-increasing degrees; only the hubs' offsets reach the host
-    const int32_t thr[7] = {t.big_max, std::min<int32_t>(kBigSplit, t.big_max), t.mid_max, 32, 16, t.tiny_max, 0};
-    int32_t b[7];
-    if ((rc = device_bounds(g, thr, 7, b))) return rc;
-    b[1] = std::min(std::max(b[1], b[0]), b[2]);
+    const int32_t thr[8] = {t.big_max, std::min<int32_t>(kBigTopSplit, t.big_max),
+                            std::min<int32_t>(kBigSplit, t.big_max), t.mid_max, 32, 16, t.tiny_max, 0};
+    int32_t b[8];
+    if ((rc = device_bounds(g, thr, 8, b))) return rc;
+    b[1] = std::min(std::max(b[1], b[0]), b[3]);
+    b[2] = std::min(std::max(b[2], b[1]), b[3]);
     std::vector<int32_t> hub_off((size_t)b[0] + 1);
     GLP_CUDA(cudaMemcpy(hub_off.data(), g->d_off, sizeof(int32_t) * hub_off.size(), cudaMemcpyDeviceToHost));
     build_host_plan(hub_off.data(), b[0], t, &hp);  // all of them are hubs
-    p.big_hi = range_verts(b[0], b[1]);
-    p.big_lo = range_verts(b[1], b[2]);
-    p.big = range_verts(b[0], b[2]);
-    p.mid = range_verts(b[2], b[3]);
-    p.mb = range_verts(b[0], b[3]);
-    p.g32 = range_verts(b[3], b[4]);
-    p.g16 = range_verts(b[4], b[5]);
-    p.tiny = range_verts(b[5], b[6]);
-    p.isolated = g->n - b[6];
+    p.big_top = range_verts(b[0], b[1]);
+    p.big_hi = range_verts(b[1], b[2]);
+    p.big_lo = range_verts(b[2], b[3]);
+    p.big = range_verts(b[0], b[3]);
+    p.mid = range_verts(b[3], b[4]);
+    p.mb = range_verts(b[0], b[4]);
+    p.g32 = range_verts(b[4], b[5]);
+    p.g16 = range_verts(b[5], b[6]);
+    p.tiny = range_verts(b[6], b[7]);
+    p.isolated = g->n - b[7];
   } else {
     if ((rc = ensure_host_offsets(g))) return rc;
     build_host_plan(g->h_off.data(), g->n, t, &hp);
@@ -263,7 +266,8 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
     if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
         (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
         (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
-        (rc = upload_verts(&p, hp.big_lo, &p.big_lo)) || (rc = upload_verts(&p, hp.big_hi, &p.big_hi))) {
+        (rc = upload_verts(&p, hp.big_lo, &p.big_lo)) || (rc = upload_verts(&p, hp.big_hi, &p.big_hi)) ||
+        (rc = upload_verts(&p, hp.big_top, &p.big_top))) {
       free_plan(&p);
       return rc;
     }
@@ -395,7 +399,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   GLP_CUDA(cudaEventRecord(L.fork, s));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[0], L.fork, 0));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[1], L.fork, 0));
-  constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 512, kGroupU = 4;
+  constexpr int kMidNT = 256, kBigNT = 256, kListNT = 512, kHubNT = 512, kBucketNT = 512, kGroupU = 4;
   if (p.n_hubs) {
     const size_t sm = 2ull * kHubTable * sizeof(uint32_t);
     const size_t sm_hist = (size_t)p.hub.max_nb * sizeof(uint32_t);
@@ -431,7 +435,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     // a summary screen decides what it can over the whole tier (its work
     // lists included); the exact kernel takes the vertices it lists
     const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
-    if ((rc = allow_smem(k_big<kBigNT, W, S>, sm))) return rc;
+    if ((rc = allow_smem(k_big<kListNT, W, S>, sm))) return rc;
     if ((rc = mark_on(s, 4, 0))) return rc;
     GLP_CUDA(cudaMemsetAsync(p.fscreen.count, 0, sizeof(uint32_t), s));
     TierWork all = work(p.big, 4, &p.fbig);
@@ -444,29 +448,43 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
           a, all, score, p.fscreen);
     }
     TierWork rest{Verts{nullptr, 0, 0}, p.fscreen, FailList{nullptr, nullptr}, 0, 1};
-    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, rest, score);
+    k_big<kListNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, 148 * 2), kListNT, sm, s>>>(a, rest, score);
     *launches += 2;
     if ((rc = mark_on(s, 4, 1))) return rc;
   } else if (p.big.n) {
-    // full mode: degrees <= kBigSplit in small-table blocks, the rest with the
-    // full table; majority and frontier lists all go to the full-table launch
+    // full mode: three degree ranges, each with the table and block size it
+    // needs; outside full mode the tier's majority / frontier list goes to
+    // one launch with the full table
+    constexpr int kTopNT = 1024;
     const size_t sm_lo = 4ull * kBigSplit * sizeof(uint32_t);
+    const size_t sm_hi = 4ull * kBigTopSplit * sizeof(uint32_t);
     const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
-    if ((rc = allow_smem(k_big<kBigNT, W, S>, sm))) return rc;
+    if ((rc = allow_smem(k_big<kBigNT, W, S>, sm_hi)) || (rc = allow_smem(k_big<kTopNT, W, S>, sm)) ||
+        (rc = allow_smem(k_big<kListNT, W, S>, sm)))
+      return rc;
     if ((rc = mark_on(s, 4, 0))) return rc;
+    const FailList none{nullptr, nullptr};
     if (p.big_lo.n) {
-      TierWork lo{p.big_lo, FailList{nullptr, nullptr}, FailList{nullptr, nullptr}, 1};
+      TierWork lo{p.big_lo, none, none, 1};
       k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big_lo.n, kMaxGrid), kBigNT, sm_lo, s>>>(a, lo, score);
       ++*launches;
     }
-    TierWork hi = work(p.big_hi, 4, &p.fbig);
-    hi.front = p.front.tier[4];
-    // outside full mode this launch takes the whole tier's lists
-    const bool any_hi = p.big_hi.n > 0;
-    if (!any_hi) hi.all = Verts{nullptr, 0, 0};
-    k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), kBigNT, sm, s>>>(a, hi, score);
+    if (p.big_hi.n) {
+      TierWork hi{p.big_hi, none, none, 1};
+      k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big_hi.n, kMaxGrid), kBigNT, sm_hi, s>>>(a, hi, score);
+      ++*launches;
+    }
+    if (p.big_top.n) {
+      TierWork top{p.big_top, none, none, 1};
+      k_big<kTopNT, W, S><<<(unsigned)std::min<int64_t>(p.big_top.n, kMaxGrid), kTopNT, sm, s>>>(a, top, score);
+      ++*launches;
+    }
+    if (modal) {
+      TierWork listed = work(Verts{nullptr, 0, 0}, 4, &p.fbig);
+      k_big<kListNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, 148 * 2), kListNT, sm, s>>>(a, listed, score);
+      ++*launches;
+    }
     if ((rc = mark_on(s, 4, 1))) return rc;
-    ++*launches;
   }
   if (p.mid.n) {
     if ((rc = mark_on(s, 3, 0))) return rc;

@@ -23,15 +23,18 @@ int cuda_fail(cudaError_t e, const char* what);
 // Degree-tier parameters after defaults and limits are applied.
 // Exact-count tier limits: a mid warp's table holds kMidCap slots, a big
 // block's table kBigCap slots (both at most half full).
-constexpr int kMidCap = 512, kBigCap = 8192;
-// In full mode big vertices up to kBigSplit degrees use a block with a table
-// of 2*kBigSplit slots (more blocks per SM); the rest of the tier the full one.
-constexpr int kBigSplit = 1024;
+constexpr int kMidCap = 512, kBigCap = 16384;
+// In full mode the big tier runs as three launches: degrees up to kBigSplit
+// in 256-thread blocks with tables of 2*kBigSplit slots (several blocks per
+// SM), degrees up to kBigTopSplit in 256-thread blocks with tables of
+// 2*kBigTopSplit slots, and the rest in 1024-thread blocks with the full
+// kBigCap table (one block per SM).
+constexpr int kBigSplit = 1024, kBigTopSplit = 4096;
 
 struct TierParams {
   int32_t tiny_max = 8;       // <= 8
   int32_t mid_max = 256;      // <= kMidCap / 2
-  int32_t big_max = 4096;     // <= kBigCap / 2
+  int32_t big_max = 8192;     // <= kBigCap / 2
   int32_t hub_chunk = 16384;  // edges per hub streaming block
   bool operator==(const TierParams& o) const {
     return tiny_max == o.tiny_max && mid_max == o.mid_max && big_max == o.big_max && hub_chunk == o.hub_chunk;
@@ -42,7 +45,7 @@ int resolve_tiers(const glp_params* p, TierParams* t);
 // Host-side plan (pure function of the offsets and the tier parameters).
 struct HostPlan {
   std::vector<int32_t> tiny, g16, g32, mid, big, mb;  // vertex lists (ascending ids); mb = mid + big
-  std::vector<int32_t> big_lo, big_hi;                 // the big tier split at kBigSplit
+  std::vector<int32_t> big_lo, big_hi, big_top;        // the big tier split at kBigSplit, kBigTopSplit
   int64_t isolated = 0;
   int64_t edges[7] = {0, 0, 0, 0, 0, 0, 0};  // per tier, as the vertex counts of glp_graph_plan
   // hubs
@@ -59,7 +62,7 @@ struct DevicePlan {
   cudaStream_t setup = nullptr;  // stream of the set-up copies (the handle's)
   TierParams tiers;
   bool valid = false;
-  Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{}, big_lo{}, big_hi{};
+  Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{}, big_lo{}, big_hi{}, big_top{};
   FailList fmid{}, fbig{};
   FailList fscreen{};  // big-tier vertices a summary screen left to the exact kernel
   // list counters: [majority mid, majority big, frontier tiny, g16, g32, mid,

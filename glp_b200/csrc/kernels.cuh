@@ -12,8 +12,8 @@
 //   tiny  (1..8)       : one thread per vertex, labels in registers
 //   group (9..32)      : 16 or 32 lanes per vertex, one __match_any_sync round
 //   mid   (33..256)    : one warp per vertex, per-warp shared-memory table
-//   big   (257..4096)  : one block per vertex, block shared-memory table
-//   hub   (> 4096)     : labels gathered once and sorted into hash buckets,
+//   big   (257..8192)  : one block per vertex, block shared-memory table
+//   hub   (> 8192)     : labels gathered once and sorted into hash buckets,
 //                        one block per (hub, bucket) with a shared table
 // Majority shortcut (classic, weighted, SLPA listener): when a vertex's own
 // label holds more than half of its neighbourhood weight it is the unique
@@ -387,7 +387,7 @@ __device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t*
 }
 
 // ---------------------------------------------------- majority pre-pass
-// One warp per vertex of degree 33..4096: count the weight of the vertex's
+// One warp per vertex of degree 33..8192: count the weight of the vertex's
 // own label with 4 independent column/label loads in flight per lane.  A
 // strict majority is written; other vertices go to the mid or big fail list.
 template <bool W>

@@ -85,7 +85,7 @@ typedef struct glp_params {
   /* degree tiers (0 = engine default / autotuned) */
   int32_t tiny_max;               /* thread per vertex up to this degree (<= 8) */
   int32_t mid_max;                /* warp per vertex up to this degree (32..256) */
-  int32_t big_max;                /* block per vertex up to this degree (mid_max..4096); above: hubs */
+  int32_t big_max;                /* block per vertex up to this degree (mid_max..8192); above: hubs */
   int32_t hub_chunk;              /* edges per hub streaming block (256..65536) */
   int32_t use_graph;              /* capture the iteration loop in a CUDA graph */
   int32_t async;                  /* 1: enqueue on the stream and return without
