@@ -15,6 +15,9 @@ the device-resident graph.  GTEPS = CSR entries x iterations / seconds.
   the labels back into a pinned host buffer.
 * roofline: the dominant kernel tier, algorithmic bytes 8*m_t + 12*n_t per
   launch over its CUDA-event launch time, against the measured HBM copy peak.
+  Tier times come from PROFILE_RUNS further runs after the timed region, with
+  the step's kernels on one stream so that each tier's events bracket only
+  its own kernels (the timed runs overlap tiers on three streams).
 * cpu_baseline: the reference's own OpenMP CPU path (tutorial/CPUlp.cuh,
   compiled from source into oracle/_ref) on the same graph, one iteration.
 
@@ -44,6 +47,7 @@ import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
 ITERS = 20
+PROFILE_RUNS = 3  # untimed runs with per-tier CUDA events (roofline, tier times)
 TIER_NAMES = ("tiny", "group16", "group32", "mid", "big", "hub", "aux", "majority")
 TIER_PLAN_KEYS = {0: "tiny", 1: "group16", 2: "group32", 3: "mid", 4: "big", 5: "hub"}
 
@@ -309,14 +313,25 @@ def run_glp(args, ws, rank, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        r = handle.run(_lib.METHOD_CLASSIC, args.iters, params, labels_out=labels_dev, stream=sp, profile=True)
-        tier_ms += r.tier_ms
+        r = handle.run(_lib.METHOD_CLASSIC, args.iters, params, labels_out=labels_dev, stream=sp)
         launches += r.launches
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     barrier(ws)
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
+    # per-tier kernel times, outside the timed region: the same run with every
+    # kernel of a step on one stream (GLP_SERIAL_STEP=1), so that a tier's
+    # CUDA-event time is its kernels' own duration, not a span shared with
+    # the tiers running beside it
+    os.environ["GLP_SERIAL_STEP"] = "1"
+    try:
+        for _ in range(PROFILE_RUNS):
+            r = handle.run(_lib.METHOD_CLASSIC, args.iters, params, labels_out=labels_dev, stream=sp, profile=True)
+            tier_ms += r.tier_ms
+    finally:
+        os.environ.pop("GLP_SERIAL_STEP", None)
+    torch.cuda.synchronize(dev)
     ms_max = max_over_ranks(ws, ms)
     edges_total = sum_over_ranks(ws, float(m) * args.iters * args.steps)
     value = edges_total / (ms_max / 1e3) / 1e9
@@ -348,7 +363,7 @@ def run_glp(args, ws, rank, local):
 
     # roofline of the dominant kernel tier
     peak, peak_kind = measured_peak()
-    launches_per_tier = args.steps * args.iters
+    launches_per_tier = PROFILE_RUNS * args.iters
     dom = max(TIER_PLAN_KEYS, key=lambda i: tier_ms[i])
     key = TIER_PLAN_KEYS[dom]
     n_t, m_t = plan[f"v_{key}"], plan[f"e_{key}"]  # vertices and CSR entries of that kernel group

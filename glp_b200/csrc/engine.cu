@@ -352,13 +352,12 @@ static int allow_smem(K kernel, size_t bytes) {
 
 static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// GLP_SERIAL_STEP=1 keeps every kernel of a step on one stream (profiling).
+// GLP_SERIAL_STEP=1 (read at every step) keeps every kernel of a step on one
+// stream, so that per-tier CUDA-event times are the kernels' own durations
+// instead of spans that overlap other tiers (profiling).
 static bool serial_step() {
-  static const bool on = [] {
-    const char* e = std::getenv("GLP_SERIAL_STEP");
-    return e && e[0] == '1';
-  }();
-  return on;
+  const char* e = std::getenv("GLP_SERIAL_STEP");
+  return e && e[0] == '1';
 }
 
 template <bool W, class S>
