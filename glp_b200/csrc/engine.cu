@@ -148,7 +148,9 @@ void build_host_plan(const int32_t* off, int32_t n, const TierParams& t, HostPla
     } else if (d <= t.big_max) {
       hp->big.push_back(v);
       hp->mb.push_back(v);
-      (d <= kBigSplit ? hp->big_lo : d <= kBigTopSplit ? hp->big_hi : hp->big_top).push_back(v);
+      int r = 0;
+      while (r + 1 < kBigParts && d > kBigPartMax[r]) ++r;
+      hp->big_part[r].push_back(v);
       tier = 5;
     } else {
       tier = 6;
@@ -240,25 +242,31 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   if (g->deg_sorted == 1) {
     // every tier is a contiguous range: its bounds come from binary searches
     // over the non-increasing degrees; only the hubs' offsets reach the host
-    const int32_t thr[8] = {t.big_max, std::min<int32_t>(kBigTopSplit, t.big_max),
-                            std::min<int32_t>(kBigSplit, t.big_max), t.mid_max, 32, 16, t.tiny_max, 0};
-    int32_t b[8];
-    if ((rc = device_bounds(g, thr, 8, b))) return rc;
-    b[1] = std::min(std::max(b[1], b[0]), b[3]);
-    b[2] = std::min(std::max(b[2], b[1]), b[3]);
+    // thresholds, descending: big_max, the part bounds below it, mid_max, 32,
+    // 16, tiny_max, 0; b[i] = vertices of degree > thr[i]
+    constexpr int kT = kBigParts + 5;
+    int32_t thr[kT];
+    thr[0] = t.big_max;
+    for (int r = kBigParts - 2, i = 1; r >= 0; --r, ++i) thr[i] = std::min<int32_t>(kBigPartMax[r], t.big_max);
+    thr[kBigParts] = t.mid_max;
+    thr[kBigParts + 1] = 32;
+    thr[kBigParts + 2] = 16;
+    thr[kBigParts + 3] = t.tiny_max;
+    thr[kBigParts + 4] = 0;
+    int32_t b[kT];
+    if ((rc = device_bounds(g, thr, kT, b))) return rc;
+    for (int i = 1; i < kBigParts; ++i) b[i] = std::min(std::max(b[i], b[i - 1]), b[kBigParts]);
     std::vector<int32_t> hub_off((size_t)b[0] + 1);
     GLP_CUDA(cudaMemcpy(hub_off.data(), g->d_off, sizeof(int32_t) * hub_off.size(), cudaMemcpyDeviceToHost));
     build_host_plan(hub_off.data(), b[0], t, &hp);  // all of them are hubs
-    p.big_top = range_verts(b[0], b[1]);
-    p.big_hi = range_verts(b[1], b[2]);
-    p.big_lo = range_verts(b[2], b[3]);
-    p.big = range_verts(b[0], b[3]);
-    p.mid = range_verts(b[3], b[4]);
-    p.mb = range_verts(b[0], b[4]);
-    p.g32 = range_verts(b[4], b[5]);
-    p.g16 = range_verts(b[5], b[6]);
-    p.tiny = range_verts(b[6], b[7]);
-    p.isolated = g->n - b[7];
+    for (int r = 0; r < kBigParts; ++r) p.big_part[r] = range_verts(b[kBigParts - 1 - r], b[kBigParts - r]);
+    p.big = range_verts(b[0], b[kBigParts]);
+    p.mid = range_verts(b[kBigParts], b[kBigParts + 1]);
+    p.mb = range_verts(b[0], b[kBigParts + 1]);
+    p.g32 = range_verts(b[kBigParts + 1], b[kBigParts + 2]);
+    p.g16 = range_verts(b[kBigParts + 2], b[kBigParts + 3]);
+    p.tiny = range_verts(b[kBigParts + 3], b[kBigParts + 4]);
+    p.isolated = g->n - b[kBigParts + 4];
   } else {
     if ((rc = ensure_host_offsets(g))) return rc;
     build_host_plan(g->h_off.data(), g->n, t, &hp);
@@ -266,8 +274,10 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
     if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
         (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
         (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
-        (rc = upload_verts(&p, hp.big_lo, &p.big_lo)) || (rc = upload_verts(&p, hp.big_hi, &p.big_hi)) ||
-        (rc = upload_verts(&p, hp.big_top, &p.big_top))) {
+        (rc = upload_verts(&p, hp.big_part[0], &p.big_part[0])) ||
+        (rc = upload_verts(&p, hp.big_part[1], &p.big_part[1])) ||
+        (rc = upload_verts(&p, hp.big_part[2], &p.big_part[2])) ||
+        (rc = upload_verts(&p, hp.big_part[3], &p.big_part[3]))) {
       free_plan(&p);
       return rc;
     }
@@ -451,31 +461,27 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     *launches += 2;
     if ((rc = mark_on(s, 4, 1))) return rc;
   } else if (p.big.n) {
-    // full mode: three degree ranges, each with the table and block size it
-    // needs; outside full mode the tier's majority / frontier list goes to
-    // one launch with the full table
-    constexpr int kTopNT = 1024;
-    const size_t sm_lo = 4ull * kBigSplit * sizeof(uint32_t);
-    const size_t sm_hi = 4ull * kBigTopSplit * sizeof(uint32_t);
+    // full mode: one launch per degree range, each with the table and block
+    // size it needs; outside full mode the tier's majority / frontier list
+    // goes to one launch with the full table
     const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
-    if ((rc = allow_smem(k_big<kBigNT, W, S>, sm_hi)) || (rc = allow_smem(k_big<kTopNT, W, S>, sm)) ||
-        (rc = allow_smem(k_big<kListNT, W, S>, sm)))
+    if ((rc = allow_smem(k_big<256, W, S>, 4ull * kBigPartMax[1] * sizeof(uint32_t))) ||
+        (rc = allow_smem(k_big<512, W, S>, sm)) || (rc = allow_smem(k_big<1024, W, S>, sm)))
       return rc;
     if ((rc = mark_on(s, 4, 0))) return rc;
     const FailList none{nullptr, nullptr};
-    if (p.big_lo.n) {
-      TierWork lo{p.big_lo, none, none, 1};
-      k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big_lo.n, kMaxGrid), kBigNT, sm_lo, s>>>(a, lo, score);
-      ++*launches;
-    }
-    if (p.big_hi.n) {
-      TierWork hi{p.big_hi, none, none, 1};
-      k_big<kBigNT, W, S><<<(unsigned)std::min<int64_t>(p.big_hi.n, kMaxGrid), kBigNT, sm_hi, s>>>(a, hi, score);
-      ++*launches;
-    }
-    if (p.big_top.n) {
-      TierWork top{p.big_top, none, none, 1};
-      k_big<kTopNT, W, S><<<(unsigned)std::min<int64_t>(p.big_top.n, kMaxGrid), kTopNT, sm, s>>>(a, top, score);
+    static_assert(kBigParts == 4 && kBigPartThreads[0] == 256 && kBigPartThreads[1] == 256 &&
+                      kBigPartThreads[2] == 512 && kBigPartThreads[3] == 1024,
+                  "the launches below follow kBigPartThreads");
+    for (int r = 0; r < kBigParts; ++r) {
+      const Verts& vs = p.big_part[r];
+      if (!vs.n) continue;
+      const TierWork tw{vs, none, none, 1};
+      const size_t smr = 4ull * kBigPartMax[r] * sizeof(uint32_t);
+      const unsigned grid = (unsigned)std::min<int64_t>(vs.n, kMaxGrid);
+      if (kBigPartThreads[r] == 256) k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
+      else if (kBigPartThreads[r] == 512) k_big<512, W, S><<<grid, 512, smr, s>>>(a, tw, score);
+      else k_big<1024, W, S><<<grid, 1024, smr, s>>>(a, tw, score);
       ++*launches;
     }
     if (modal) {

@@ -24,12 +24,13 @@ int cuda_fail(cudaError_t e, const char* what);
 // Exact-count tier limits: a mid warp's table holds kMidCap slots, a big
 // block's table kBigCap slots (both at most half full).
 constexpr int kMidCap = 512, kBigCap = 16384;
-// In full mode the big tier runs as three launches: degrees up to kBigSplit
-// in 256-thread blocks with tables of 2*kBigSplit slots (several blocks per
-// SM), degrees up to kBigTopSplit in 256-thread blocks with tables of
-// 2*kBigTopSplit slots, and the rest in 1024-thread blocks with the full
-// kBigCap table (one block per SM).
-constexpr int kBigSplit = 1024, kBigTopSplit = 4096;
+// In full mode the big tier runs as one launch per degree range: range r
+// holds degrees up to kBigPartMax[r] (and above the previous range), counted
+// by kBigPartThreads[r]-thread blocks whose tables hold 2*kBigPartMax[r]
+// slots, so that a range's table fits as many blocks per SM as it can.
+constexpr int kBigParts = 4;
+constexpr int kBigPartMax[kBigParts] = {1024, 2048, 4096, 8192};
+constexpr int kBigPartThreads[kBigParts] = {256, 256, 512, 1024};
 
 struct TierParams {
   int32_t tiny_max = 8;       // <= 8
@@ -45,7 +46,7 @@ int resolve_tiers(const glp_params* p, TierParams* t);
 // Host-side plan (pure function of the offsets and the tier parameters).
 struct HostPlan {
   std::vector<int32_t> tiny, g16, g32, mid, big, mb;  // vertex lists (ascending ids); mb = mid + big
-  std::vector<int32_t> big_lo, big_hi, big_top;        // the big tier split at kBigSplit, kBigTopSplit
+  std::vector<int32_t> big_part[kBigParts];            // the big tier by kBigPartMax range
   int64_t isolated = 0;
   int64_t edges[7] = {0, 0, 0, 0, 0, 0, 0};  // per tier, as the vertex counts of glp_graph_plan
   // hubs
@@ -62,7 +63,7 @@ struct DevicePlan {
   cudaStream_t setup = nullptr;  // stream of the set-up copies (the handle's)
   TierParams tiers;
   bool valid = false;
-  Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{}, big_lo{}, big_hi{}, big_top{};
+  Verts tiny{}, g16{}, g32{}, mid{}, big{}, mb{}, big_part[kBigParts]{};
   FailList fmid{}, fbig{};
   FailList fscreen{};  // big-tier vertices a summary screen left to the exact kernel
   // list counters: [majority mid, majority big, frontier tiny, g16, g32, mid,

@@ -178,6 +178,9 @@ struct TierWork {
 // majority shortcut applies.
 struct ScoreClassic {
   static constexpr bool kMajority = true;
+  // (count << 32 | label) orders candidates as better() does: a block can
+  // reduce with one 64-bit shared atomicMax
+  static constexpr bool kPacked = true;
   static constexpr bool kScan = false;  // no lookup: running maximum at every insert
   __device__ __forceinline__ int64_t operator()(int32_t, uint32_t k) const { return (int64_t)k; }
   __device__ __forceinline__ int32_t vol_of(int32_t) const { return 0; }
@@ -190,6 +193,7 @@ struct ScoreClassic {
 // The volume term breaks the majority argument: no shortcut.
 struct ScoreLayered {
   static constexpr bool kMajority = false;
+  static constexpr bool kPacked = false;  // signed 64-bit scores: block_max
   // the volume is a global lookup per label: prefetched per insert, or (step
   // mode word 1) looked up once per distinct label by a scan of the table
   static constexpr bool kScan = true;
@@ -528,6 +532,10 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
   __shared__ int32_t cbuf[64];  // changed vertices not yet listed (thread 0's)
   uint32_t ncb = 0;
   __shared__ Best red[32];
+  // packed scores: one slot per vertex parity, so thread 0 can read vertex
+  // i's result while the block already counts vertex i+1 into the other
+  __shared__ unsigned long long sbest[2];
+  int par = 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
@@ -538,6 +546,7 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
     uint32_t* keys = smem;
     uint32_t* vals = smem + cap;
     zero_words16(smem, 2 * cap, threadIdx.x, NT);  // degree > 32: cap >= 128
+    if (S::kPacked && threadIdx.x == 0) sbest[par] = 0ull;
     __syncthreads();
     Best best = best_none();
     bool fail = false;
@@ -565,7 +574,17 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
       __syncthreads();
       scan_table(keys, vals, cap, threadIdx.x, NT, score, best);
     }
-    best = block_max<NT>(best, red);
+    if (S::kPacked) {
+      // counts and labels are non-negative: (count << 32 | label) is monotone
+      best = group_max<32>(best);
+      if (lane == 0 && best.l >= 0)
+        atomicMax(&sbest[par], ((unsigned long long)best.s << 32) | (uint32_t)best.l);
+      __syncthreads();
+      if (threadIdx.x == 0) best.l = (int32_t)(uint32_t)sbest[par];
+      par ^= 1;
+    } else {
+      best = block_max<NT>(best, red);
+    }
     if (threadIdx.x == 0) {
       a.lout[v] = best.l;
       if (best.l != a.lcur[v]) {
