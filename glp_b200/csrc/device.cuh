@@ -12,7 +12,15 @@ enum : uint32_t {
   kErrProbe = 1u,       // a hash table probe ran past its capacity
   kErrScoreRange = 2u,  // a layered score left the packable range
   kErrHubPlan = 4u,     // hub chunk bookkeeping inconsistent
+  kErrTable = 8u,       // a vertex's table would not fit the launch's shared memory
 };
+
+// Dynamic shared memory of the running launch, in bytes.
+__device__ __forceinline__ uint32_t dynamic_smem_bytes() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+  return r;
+}
 
 // Murmur3 fmix32 finaliser; the reference hashes labels with it too
 // (method/hashtable.cuh:19-26).
@@ -119,7 +127,20 @@ struct CountTable {
 // odd stride from other bits of the same product, so the lanes of a warp
 // finish their probes close together and the table can be half full.
 // Optionally appends newly claimed slots to `claimed`.
+// C16: counts are 16-bit, two slots to a word (slot h in half h & 1 of word
+// h >> 1), for tables whose every count stays below 2^16.
 constexpr uint32_t kNoSlot = 0xffffffffu;
+template <bool C16>
+__device__ __forceinline__ uint32_t count_add(uint32_t* vals, uint32_t h, uint32_t c) {
+  if (!C16) return atomicAdd(&vals[h], c) + c;
+  const uint32_t sh = (h & 1u) * 16u;
+  return ((atomicAdd(&vals[h >> 1], c << sh) >> sh) & 0xffffu) + c;
+}
+template <bool C16>
+__device__ __forceinline__ uint32_t count_at(const uint32_t* vals, uint32_t h) {
+  return C16 ? (vals[h >> 1] >> ((h & 1u) * 16u)) & 0xffffu : vals[h];
+}
+template <bool C16 = false>
 __device__ __forceinline__ uint32_t table_insert_bounded(uint32_t* keys, uint32_t* vals, uint32_t mask, uint32_t key,
                                                          uint32_t c, uint32_t max_probe, uint32_t* claimed,
                                                          uint32_t* nclaimed) {
@@ -128,14 +149,14 @@ __device__ __forceinline__ uint32_t table_insert_bounded(uint32_t* keys, uint32_
   uint32_t step = 0;
   for (uint32_t probe = 0; probe < max_probe; ++probe) {
     const uint32_t cur = keys[h];
-    if (cur == key) return atomicAdd(&vals[h], c) + c;
+    if (cur == key) return count_add<C16>(vals, h, c);
     if (cur == 0) {
       const uint32_t prev = atomicCAS(&keys[h], 0u, key);
       if (prev == 0u) {
         if (claimed) claimed[atomicAdd(nclaimed, 1u)] = h;
-        return atomicAdd(&vals[h], c) + c;
+        return count_add<C16>(vals, h, c);
       }
-      if (prev == key) return atomicAdd(&vals[h], c) + c;
+      if (prev == key) return count_add<C16>(vals, h, c);
     }
     if (step == 0) {
       step = ((hk >> 9) | 1u) & mask;

@@ -99,7 +99,10 @@ int resolve_tiers(const glp_params* p, TierParams* t) {
     if (p->tiny_max > 0) d.tiny_max = p->tiny_max;
     if (p->tiny_max < 0) d.tiny_max = 0;
     if (p->mid_max > 0) d.mid_max = p->mid_max;
-    if (p->big_max > 0) d.big_max = p->big_max;
+    if (p->big_max > 0) {
+      d.big_max = p->big_max;
+      d.big_auto = false;
+    }
     if (p->hub_chunk > 0) d.hub_chunk = p->hub_chunk;
   }
   if (d.tiny_max > 8) {
@@ -110,8 +113,8 @@ int resolve_tiers(const glp_params* p, TierParams* t) {
     set_error("mid_max %d outside [32, %d]", d.mid_max, kMidCap / 2);
     return GLP_EINVAL;
   }
-  if (d.big_max < d.mid_max || d.big_max > kBigCap / 2) {
-    set_error("big_max %d outside [mid_max, %d]", d.big_max, kBigCap / 2);
+  if (d.big_max < d.mid_max || d.big_max > kBigMaxUnweighted) {
+    set_error("big_max %d outside [mid_max, %d]", d.big_max, kBigMaxUnweighted);
     return GLP_EINVAL;
   }
   if (d.hub_chunk < 256 || d.hub_chunk > 65536) {
@@ -119,6 +122,19 @@ int resolve_tiers(const glp_params* p, TierParams* t) {
     return GLP_EINVAL;
   }
   *t = d;
+  return GLP_OK;
+}
+
+int tiers_for_graph(const glp_params* p, bool weighted, TierParams* t) {
+  int rc = resolve_tiers(p, t);
+  if (rc) return rc;
+  if (t->big_auto) {
+    t->big_max = weighted ? kBigMaxWeighted : kBigMaxUnweighted;
+  } else if (weighted && t->big_max > kBigMaxWeighted) {
+    set_error("big_max %d above %d needs an unweighted graph (16-bit counts)", t->big_max, kBigMaxWeighted);
+    return GLP_EINVAL;
+  }
+  static_assert(kBigMaxWeighted <= kBigCap / 2, "weighted big tables hold 2*degree slots");
   return GLP_OK;
 }
 
@@ -273,14 +289,15 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
     p.isolated = hp.isolated;
     if ((rc = upload_verts(&p, hp.tiny, &p.tiny)) || (rc = upload_verts(&p, hp.g16, &p.g16)) ||
         (rc = upload_verts(&p, hp.g32, &p.g32)) || (rc = upload_verts(&p, hp.mid, &p.mid)) ||
-        (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb)) ||
-        (rc = upload_verts(&p, hp.big_part[0], &p.big_part[0])) ||
-        (rc = upload_verts(&p, hp.big_part[1], &p.big_part[1])) ||
-        (rc = upload_verts(&p, hp.big_part[2], &p.big_part[2])) ||
-        (rc = upload_verts(&p, hp.big_part[3], &p.big_part[3]))) {
+        (rc = upload_verts(&p, hp.big, &p.big)) || (rc = upload_verts(&p, hp.mb, &p.mb))) {
       free_plan(&p);
       return rc;
     }
+    for (int r = 0; r < kBigParts; ++r)
+      if ((rc = upload_verts(&p, hp.big_part[r], &p.big_part[r]))) {
+        free_plan(&p);
+        return rc;
+      }
   }
   n_mid = p.mid.n;
   n_big = p.big.n;
@@ -370,6 +387,28 @@ static bool serial_step() {
   return e && e[0] == '1';
 }
 
+// One launch over a device-built list of big-tier vertices (majority
+// failures, frontier members, screen fallbacks): 512-thread blocks with a
+// table for the tier's largest degree (16-bit counts when the tier reaches
+// past kBigMaxWeighted).
+template <bool W, class S>
+static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWork& tw, const S& score,
+                           cudaStream_t s) {
+  const unsigned grid = (unsigned)std::min<int64_t>(p.big.n, 148 * 2);
+  if constexpr (!W) {
+    if (p.big_part[kBigParts - 1].n) {
+      const size_t sm16 = (size_t)kBig16Slots * 6;
+      GLP_CUDA(raise_smem_limit((const void*)k_big<512, false, S, true>, sm16));
+      k_big<512, false, S, true><<<grid, 512, sm16, s>>>(a, tw, score);
+      return GLP_OK;
+    }
+  }
+  const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
+  GLP_CUDA(raise_smem_limit((const void*)k_big<512, W, S>, sm));
+  k_big<512, W, S><<<grid, 512, sm, s>>>(a, tw, score);
+  return GLP_OK;
+}
+
 template <bool W, class S>
 int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_t* launches) {
   StepLaunch L = Lin;
@@ -408,7 +447,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   GLP_CUDA(cudaEventRecord(L.fork, s));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[0], L.fork, 0));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[1], L.fork, 0));
-  constexpr int kMidNT = 256, kBigNT = 256, kListNT = 512, kHubNT = 512, kBucketNT = 512, kGroupU = 4;
+  constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 512, kGroupU = 4;
   if (p.n_hubs) {
     const size_t sm = 2ull * kHubTable * sizeof(uint32_t);
     const size_t sm_hist = (size_t)p.hub.max_nb * sizeof(uint32_t);
@@ -443,8 +482,6 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   if (p.big.n && L.backend != GLP_BACKEND_EXACT) {
     // a summary screen decides what it can over the whole tier (its work
     // lists included); the exact kernel takes the vertices it lists
-    const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
-    if ((rc = allow_smem(k_big<kListNT, W, S>, sm))) return rc;
     if ((rc = mark_on(s, 4, 0))) return rc;
     GLP_CUDA(cudaMemsetAsync(p.fscreen.count, 0, sizeof(uint32_t), s));
     TierWork all = work(p.big, 4, &p.fbig);
@@ -457,21 +494,17 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
           a, all, score, p.fscreen);
     }
     TierWork rest{Verts{nullptr, 0, 0}, p.fscreen, FailList{nullptr, nullptr}, 0, 1};
-    k_big<kListNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, 148 * 2), kListNT, sm, s>>>(a, rest, score);
+    if ((rc = launch_big_list<W, S>(p, a, rest, score, s))) return rc;
     *launches += 2;
     if ((rc = mark_on(s, 4, 1))) return rc;
   } else if (p.big.n) {
     // full mode: one launch per degree range, each with the table and block
     // size it needs; outside full mode the tier's majority / frontier list
-    // goes to one launch with the full table
-    const size_t sm = 2ull * kBigCap * sizeof(uint32_t);
-    if ((rc = allow_smem(k_big<256, W, S>, 4ull * kBigPartMax[1] * sizeof(uint32_t))) ||
-        (rc = allow_smem(k_big<512, W, S>, sm)) || (rc = allow_smem(k_big<1024, W, S>, sm)))
-      return rc;
+    // goes to one launch with a table for any degree of the tier
     if ((rc = mark_on(s, 4, 0))) return rc;
     const FailList none{nullptr, nullptr};
-    static_assert(kBigParts == 4 && kBigPartThreads[0] == 256 && kBigPartThreads[1] == 256 &&
-                      kBigPartThreads[2] == 512 && kBigPartThreads[3] == 1024,
+    static_assert(kBigParts == 5 && kBigPartThreads[0] == 256 && kBigPartThreads[1] == 256 &&
+                      kBigPartThreads[2] == 512 && kBigPartThreads[3] == 1024 && kBigPartThreads[4] == 1024,
                   "the launches below follow kBigPartThreads");
     for (int r = 0; r < kBigParts; ++r) {
       const Verts& vs = p.big_part[r];
@@ -479,14 +512,26 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       const TierWork tw{vs, none, none, 1};
       const size_t smr = 4ull * kBigPartMax[r] * sizeof(uint32_t);
       const unsigned grid = (unsigned)std::min<int64_t>(vs.n, kMaxGrid);
-      if (kBigPartThreads[r] == 256) k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
-      else if (kBigPartThreads[r] == 512) k_big<512, W, S><<<grid, 512, smr, s>>>(a, tw, score);
-      else k_big<1024, W, S><<<grid, 1024, smr, s>>>(a, tw, score);
+      if (r < 2) {
+        k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
+      } else if (r == 2) {
+        if ((rc = allow_smem(k_big<512, W, S>, smr))) return rc;
+        k_big<512, W, S><<<grid, 512, smr, s>>>(a, tw, score);
+      } else if (r == 3) {
+        if ((rc = allow_smem(k_big<1024, W, S>, smr))) return rc;
+        k_big<1024, W, S><<<grid, 1024, smr, s>>>(a, tw, score);
+      } else if constexpr (!W) {  // the 16-bit range: unweighted graphs only
+        const size_t sm16 = (size_t)kBig16Slots * 6;
+        if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
+        k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
+      } else {
+        set_error("weighted graph with big-tier degrees above %d", kBigMaxWeighted);
+        return GLP_EINVAL;
+      }
       ++*launches;
     }
     if (modal) {
-      TierWork listed = work(Verts{nullptr, 0, 0}, 4, &p.fbig);
-      k_big<kListNT, W, S><<<(unsigned)std::min<int64_t>(p.big.n, 148 * 2), kListNT, sm, s>>>(a, listed, score);
+      if ((rc = launch_big_list<W, S>(p, a, work(Verts{nullptr, 0, 0}, 4, &p.fbig), score, s))) return rc;
       ++*launches;
     }
     if ((rc = mark_on(s, 4, 1))) return rc;
@@ -632,7 +677,8 @@ static int check_err(glp_graph* g, cudaStream_t s) {
   if (err) {
     GLP_CUDA(cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), s));
     GLP_CUDA(cudaStreamSynchronize(s));
-    set_error("kernel error flags 0x%x (probe overflow=1, score range=2, hub plan=4)", err);
+    set_error("kernel error flags 0x%x (probe overflow=1, score range=2, hub plan=4, table past shared memory=8)",
+              err);
     return GLP_EKERNEL;
   }
   return GLP_OK;
@@ -1256,6 +1302,8 @@ int glp_graph_info(const glp_graph* g, int32_t* n, int64_t* m, int32_t* max_degr
   return GLP_OK;
 }
 
+static int plan_counts(const int32_t* offsets, int32_t n, const TierParams& t, int64_t out[16]);
+
 int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int64_t out[16]) {
   if (!offsets || !out || n < 0) {
     set_error("NULL argument or n < 0");
@@ -1267,8 +1315,12 @@ int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int
       return GLP_EINVAL;
     }
   TierParams t;
-  int rc = resolve_tiers(p, &t);
+  int rc = tiers_for_graph(p, false, &t);
   if (rc) return rc;
+  return plan_counts(offsets, n, t, out);
+}
+
+static int plan_counts(const int32_t* offsets, int32_t n, const TierParams& t, int64_t out[16]) {
   HostPlan hp;
   build_host_plan(offsets, n, t, &hp);
   out[0] = hp.isolated;
@@ -1289,9 +1341,14 @@ int glp_graph_plan(glp_graph* g, const glp_params* p, int64_t out[16]) {
     set_error("graph is NULL");
     return GLP_EINVAL;
   }
-  int rc = ensure_host_offsets(g);
-  if (rc) return rc;
-  return glp_plan_offsets(g->h_off.data(), g->n, p, out);
+  if (!out) {
+    set_error("out is NULL");
+    return GLP_EINVAL;
+  }
+  TierParams t;
+  int rc = tiers_for_graph(p, g->d_w != nullptr, &t);
+  if (rc || (rc = ensure_host_offsets(g))) return rc;
+  return plan_counts(g->h_off.data(), g->n, t, out);
 }
 
 int glp_graph_check(glp_graph* g) {
@@ -1466,7 +1523,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
     return GLP_EINVAL;
   }
   TierParams t;
-  int rc = resolve_tiers(&p, &t);
+  int rc = tiers_for_graph(&p, g->d_w != nullptr, &t);
   if (rc) return rc;
   if (g->n == 0) {
     if (out->changed)

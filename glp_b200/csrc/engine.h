@@ -28,20 +28,27 @@ constexpr int kMidCap = 512, kBigCap = 16384;
 // holds degrees up to kBigPartMax[r] (and above the previous range), counted
 // by kBigPartThreads[r]-thread blocks whose tables hold 2*kBigPartMax[r]
 // slots, so that a range's table fits as many blocks per SM as it can.
-constexpr int kBigParts = 4;
-constexpr int kBigPartMax[kBigParts] = {1024, 2048, 4096, 8192};
-constexpr int kBigPartThreads[kBigParts] = {256, 256, 512, 1024};
+// The last range counts with 16-bit counts (k_big<..., C16>), so it exists
+// for unweighted graphs only: weighted graphs cap big_max at
+// kBigMaxWeighted.
+constexpr int kBigParts = 5;
+constexpr int kBigPartMax[kBigParts] = {1024, 2048, 4096, 8192, 24576};
+constexpr int kBigPartThreads[kBigParts] = {256, 256, 512, 1024, 1024};
+constexpr int kBigMaxWeighted = 8192, kBigMaxUnweighted = 24576;
 
 struct TierParams {
   int32_t tiny_max = 8;       // <= 8
   int32_t mid_max = 256;      // <= kMidCap / 2
-  int32_t big_max = 8192;     // <= kBigCap / 2
+  int32_t big_max = kBigMaxWeighted;  // <= kBigMaxUnweighted (unweighted graphs), <= kBigCap / 2 (weighted)
+  bool big_auto = true;               // big_max not given: the largest the graph's counts allow
   int32_t hub_chunk = 16384;  // edges per hub streaming block
   bool operator==(const TierParams& o) const {
     return tiny_max == o.tiny_max && mid_max == o.mid_max && big_max == o.big_max && hub_chunk == o.hub_chunk;
   }
 };
 int resolve_tiers(const glp_params* p, TierParams* t);
+// resolve_tiers, then big_max for a graph with (weighted) or without weights.
+int tiers_for_graph(const glp_params* p, bool weighted, TierParams* t);
 
 // Host-side plan (pure function of the offsets and the tier parameters).
 struct HostPlan {

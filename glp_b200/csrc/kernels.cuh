@@ -12,8 +12,8 @@
 //   tiny  (1..8)       : one thread per vertex, labels in registers
 //   group (9..32)      : 16 or 32 lanes per vertex, one __match_any_sync round
 //   mid   (33..256)    : one warp per vertex, per-warp shared-memory table
-//   big   (257..8192)  : one block per vertex, block shared-memory table
-//   hub   (> 8192)     : labels gathered once and sorted into hash buckets,
+//   big   (257..24576) : one block per vertex, block shared-memory table
+//   hub   (above big)  : labels gathered once and sorted into hash buckets,
 //                        one block per (hub, bucket) with a shared table
 // Majority shortcut (classic, weighted, SLPA listener): when a vertex's own
 // label holds more than half of its neighbourhood weight it is the unique
@@ -366,7 +366,7 @@ __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, 
 // The best (score, label) over the occupied slots of a finished table, slots
 // t, t+stride, ... of it (scores with kScan).
 // Eight slots a round, their volume loads in flight together.
-template <class S>
+template <bool C16 = false, class S>
 __device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t* vals, uint32_t cap, uint32_t t,
                                            uint32_t stride, const S& score, Best& best) {
   constexpr int U = 8;
@@ -377,7 +377,7 @@ __device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t*
     for (int u = 0; u < U; ++u) {
       const uint32_t s = s0 + u * stride;
       key[u] = s < cap ? keys[s] : 0u;
-      val[u] = s < cap ? vals[s] : 0u;
+      val[u] = s < cap ? count_at<C16>(vals, s) : 0u;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) vl[u] = key[u] ? score.vol_of((int32_t)(key[u] - 1u)) : 0;
@@ -391,7 +391,7 @@ __device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t*
 }
 
 // ---------------------------------------------------- majority pre-pass
-// One warp per vertex of degree 33..8192: count the weight of the vertex's
+// One warp per vertex of the mid and big tiers: count the weight of the vertex's
 // own label with 4 independent column/label loads in flight per lane.  A
 // strict majority is written; other vertices go to the mid or big fail list.
 template <bool W>
@@ -523,10 +523,14 @@ __device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32
 }
 
 // ----------------------------------------------------------------- big tier
-// Exact count, one block per vertex (degree <= CAP/2): block shared table
-// (dynamic, CAP slots) sized per vertex to the power of two >= 2*degree.
-template <int NT, bool W, class S>
+// Exact count, one block per vertex: block shared table (dynamic) sized per
+// vertex to the power of two >= 2*degree.  C16 (unweighted counts only):
+// 16-bit counts, and at most kBig16Slots slots (three quarters full at
+// degree 24576), so 24576 labels fit 192 KB of shared memory.
+constexpr uint32_t kBig16Slots = 32768;
+template <int NT, bool W, class S, bool C16 = false>
 __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
+  static_assert(!(C16 && W), "16-bit counts hold unweighted counts only");
   const bool scan = S::kScan && scan_scores(a);
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ int32_t cbuf[64];  // changed vertices not yet listed (thread 0's)
@@ -542,16 +546,21 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
   for (int32_t i = blockIdx.x; i < nwork; i += gridDim.x) {
     const int32_t v = tw.at(mode, i);
     const int32_t b = a.off[v], e = a.off[v + 1];
-    const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));
+    const uint32_t cap = C16 ? min(pow2_ceil(2u * (uint32_t)(e - b)), kBig16Slots) : pow2_ceil(2u * (uint32_t)(e - b));
+    const uint32_t words = C16 ? cap + cap / 2 : 2 * cap;
+    if (4ull * words > dynamic_smem_bytes()) {  // a planning error: report it, touch nothing (block-uniform)
+      if (threadIdx.x == 0) atomicOr(a.err, kErrTable);
+      continue;
+    }
     uint32_t* keys = smem;
     uint32_t* vals = smem + cap;
-    zero_words16(smem, 2 * cap, threadIdx.x, NT);  // degree > 32: cap >= 128
+    zero_words16(smem, words, threadIdx.x, NT);  // degree > 32: cap >= 128
     if (S::kPacked && threadIdx.x == 0) sbest[par] = 0ull;
     __syncthreads();
     Best best = best_none();
     bool fail = false;
     auto ins = [&](uint32_t key, uint32_t k) {
-      return table_insert_bounded(keys, vals, cap - 1, key, k, cap, nullptr, nullptr);
+      return table_insert_bounded<C16>(keys, vals, cap - 1, key, k, cap, nullptr, nullptr);
     };
     for (int32_t j0 = b + warp * 32; j0 < e; j0 += 4 * NT) {
       int32_t lab[4];
@@ -572,7 +581,7 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {  // block-uniform
       __syncthreads();
-      scan_table(keys, vals, cap, threadIdx.x, NT, score, best);
+      scan_table<C16>(keys, vals, cap, threadIdx.x, NT, score, best);
     }
     if (S::kPacked) {
       // counts and labels are non-negative: (count << 32 | label) is monotone

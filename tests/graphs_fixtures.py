@@ -74,4 +74,4 @@ def planted_np(n, k, din, dout, seed, weighted=False):
 
 BOUNDARY_DEGREES = [1, 2, 3, 7, 8, 9, 15, 16, 17, 31, 32, 33, 63, 64, 65, 127, 128, 129, 255, 256, 257,
                     639, 640, 641, 1023, 1280, 1281, 1500, 2043, 2044, 2045, 2048, 2049, 2100, 4095, 4096, 4097, 6000, 8191,
-                    8192, 8193, 9000]
+                    8192, 8193, 9000, 16384, 16385, 24575, 24576, 24577]

@@ -69,16 +69,18 @@ def _plan(off, **kw):
 
 
 def test_planner_tiers():
-    degs = [0, 1, 8, 9, 16, 17, 32, 33, 256, 257, 4096, 4097, 8192, 8193, 10000, 20000]
+    degs = [0, 1, 8, 9, 16, 17, 32, 33, 256, 257, 4096, 4097, 8192, 8193, 10000, 20000, 24576, 24577, 30000]
     off = np.concatenate([[0], np.cumsum(degs)]).astype(np.int32)
-    rc, out = _plan(off, hub_chunk=4096)
+    rc, out = _plan(off, hub_chunk=4096)  # host offsets alone: planned as an unweighted graph
     assert rc == 0
-    assert out[:7] == [1, 2, 2, 2, 2, 4, 3]  # isolated, tiny, g16, g32, mid, big, hub
-    assert out[7] == 4 + 4 + 8  # hub hash buckets: ceil(3 * deg / 8192)
-    assert out[15] == 3 + 3 + 5  # hub streaming chunks of 4096 edges
-    assert out[9] == 9 and out[14] == 8193 + 10000 + 20000
+    assert out[:7] == [1, 2, 2, 2, 2, 8, 2]  # isolated, tiny, g16, g32, mid, big, hub
+    assert out[7] == 10 + 11  # hub hash buckets: ceil(3 * deg / 8192)
+    assert out[15] == 7 + 8  # hub streaming chunks of 4096 edges
+    assert out[9] == 9 and out[14] == 24577 + 30000
+    rc, out = _plan(off, hub_chunk=4096, big_max=8192)
+    assert rc == 0 and out[5] == 4 and out[6] == 6
     rc, out = _plan(off, tiny_max=4, mid_max=64, big_max=512, hub_chunk=256)
-    assert rc == 0 and out[1] == 1 and out[2] == 3 and out[5] == 2 and out[6] == 6
+    assert rc == 0 and out[1] == 1 and out[2] == 3 and out[5] == 2 and out[6] == 9
 
 
 def test_planner_rejects_bad_input():
@@ -88,7 +90,7 @@ def test_planner_rejects_bad_input():
     assert rc == _lib.GLP_EINVAL
     rc, out = _plan(np.array([0, 1], np.int32), mid_max=300)
     assert rc == _lib.GLP_EINVAL
-    rc, out = _plan(np.array([0, 1], np.int32), big_max=8193)
+    rc, out = _plan(np.array([0, 1], np.int32), big_max=24577)
     assert rc == _lib.GLP_EINVAL
     rc, out = _plan(np.array([0, 1], np.int32), hub_chunk=100)
     assert rc == _lib.GLP_EINVAL

@@ -259,6 +259,23 @@ def test_malformed_csr_rejected():
         Graph(from_numpy(off, np.array([1, 1, 0], np.int32), np.array([1, -2, 1], np.int32)))
 
 
+def test_big_tier_bound_depends_on_weights():
+    """Unweighted graphs count degrees up to 24576 in the big tier (16-bit
+    counts); weighted graphs stop at 8192, and reject a larger big_max."""
+    off, cols = CASES["star_ring_20000"]
+    w = np.ones(len(cols), np.int32)
+    with Graph(from_numpy(off, cols)) as g:
+        assert g.plan()["v_hub"] == 0 and g.plan()["v_big"] == 1
+    with Graph(from_numpy(off, cols, w)) as g:
+        assert g.plan()["v_hub"] == 1 and g.plan()["v_big"] == 0
+        with pytest.raises(_lib.GlpError) as e:
+            g.run(_lib.METHOD_CLASSIC, 2, make_params(big_max=9000))
+        assert e.value.code == _lib.GLP_EINVAL
+        res = g.run(_lib.METHOD_CLASSIC, 4)
+    _, otr = O.classic_run(off, cols, 4, w=w, trace=True)
+    np.testing.assert_array_equal(res.labels, otr[-1])
+
+
 def test_callback_can_stop_the_run():
     off, cols = CASES["rmat12"]
     g = Graph(from_numpy(off, cols))
