@@ -393,8 +393,9 @@ static bool serial_step() {
 // past kBigMaxWeighted).
 template <bool W, class S>
 static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWork& tw, const S& score,
-                           cudaStream_t s) {
+                           cudaStream_t s, int64_t* launches) {
   const unsigned grid = (unsigned)std::min<int64_t>(p.big.n, 148 * 2);
+  ++*launches;
   if constexpr (!W) {
     if (p.big_part[kBigParts - 1].n) {
       const size_t sm16 = (size_t)kBig16Slots * 6;
@@ -494,8 +495,8 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
           a, all, score, p.fscreen);
     }
     TierWork rest{Verts{nullptr, 0, 0}, p.fscreen, FailList{nullptr, nullptr}, 0, 1};
-    if ((rc = launch_big_list<W, S>(p, a, rest, score, s))) return rc;
-    *launches += 2;
+    if ((rc = launch_big_list<W, S>(p, a, rest, score, s, launches))) return rc;
+    ++*launches;
     if ((rc = mark_on(s, 4, 1))) return rc;
   } else if (p.big.n) {
     // full mode: one launch per degree range, each with the table and block
@@ -531,8 +532,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       ++*launches;
     }
     if (modal) {
-      if ((rc = launch_big_list<W, S>(p, a, work(Verts{nullptr, 0, 0}, 4, &p.fbig), score, s))) return rc;
-      ++*launches;
+      if ((rc = launch_big_list<W, S>(p, a, work(Verts{nullptr, 0, 0}, 4, &p.fbig), score, s, launches))) return rc;
     }
     if ((rc = mark_on(s, 4, 1))) return rc;
   }

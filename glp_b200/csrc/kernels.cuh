@@ -539,13 +539,52 @@ __global__ void __launch_bounds__(NT) k_big(StepArgs a, TierWork tw, S score) {
   // packed scores: one slot per vertex parity, so thread 0 can read vertex
   // i's result while the block already counts vertex i+1 into the other
   __shared__ unsigned long long sbest[2];
-  int par = 0;
+  __shared__ uint32_t msum[2][2];  // majority test: (own-label weight, total weight) per vertex parity
+  int par = 0, mpar = 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
   for (int32_t i = blockIdx.x; i < nwork; i += gridDim.x) {
     const int32_t v = tw.at(mode, i);
     const int32_t b = a.off[v], e = a.off[v + 1];
+    if (S::kMajority && mode == kModeFrontier) {
+      // a frontier vertex of this tier has many neighbours and usually keeps
+      // its label: a strict majority of its own label decides it without a
+      // table (the majority pre-pass does this for every tier in majority
+      // steps)
+      const int32_t cand = a.lcur[v];
+      if (threadIdx.x == 0) msum[mpar][0] = msum[mpar][1] = 0u;
+      __syncthreads();
+      uint32_t cnt = 0, tot = 0;
+      for (int32_t j0 = b + threadIdx.x; j0 < e; j0 += 4 * NT) {
+        int32_t c[4];
+        uint32_t wt[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int32_t j = j0 + q * NT;
+          c[q] = j < e ? ld_stream(a.cols + j) : -1;
+          wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          cnt += (c[q] >= 0 && ld_label(a.lin + c[q]) == cand) ? wt[q] : 0u;
+          tot += wt[q];
+        }
+      }
+      cnt = __reduce_add_sync(kFull, cnt);
+      tot = __reduce_add_sync(kFull, tot);
+      if (lane == 0) {
+        atomicAdd(&msum[mpar][0], cnt);
+        atomicAdd(&msum[mpar][1], tot);
+      }
+      __syncthreads();
+      const bool major = 2ull * msum[mpar][0] > (unsigned long long)msum[mpar][1];
+      mpar ^= 1;  // the next vertex resets the other pair while this one is read
+      if (major) {  // block-uniform
+        if (threadIdx.x == 0) a.lout[v] = cand;
+        continue;
+      }
+    }
     const uint32_t cap = C16 ? min(pow2_ceil(2u * (uint32_t)(e - b)), kBig16Slots) : pow2_ceil(2u * (uint32_t)(e - b));
     const uint32_t words = C16 ? cap + cap / 2 : 2 * cap;
     if (4ull * words > dynamic_smem_bytes()) {  // a planning error: report it, touch nothing (block-uniform)
