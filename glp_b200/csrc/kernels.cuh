@@ -229,7 +229,7 @@ __device__ __forceinline__ unsigned long long pack_best(const Best& b, uint32_t*
 
 // ---------------------------------------------------------------- tiny tier
 template <int TMAX, bool W, class S>
-__global__ void __launch_bounds__(256, (TMAX >= 32 && !W && !S::kScan) ? 2 : 1) k_tiny(StepArgs a, TierWork tw, S score) {
+__global__ void __launch_bounds__(256, TMAX >= 32 ? 2 : 1) k_tiny(StepArgs a, TierWork tw, S score) {
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
   // grid-stride over whole warps so record_changes sees full warps
@@ -250,21 +250,31 @@ __global__ void __launch_bounds__(256, (TMAX >= 32 && !W && !S::kScan) ? 2 : 1) 
       if (i < d) load_edge<W>(a, (int64_t)b + i, lab[i], wt[i]);
     }
     sort_labels<TMAX, W>(lab, wt);
-    // every label's volume (layered LP) is loaded before the scan, so the
-    // loads are in flight together
-    int32_t vl[TMAX];
-#pragma unroll
-    for (int i = 0; i < TMAX; ++i) vl[i] = (S::kScan && lab[i] != INT32_MAX) ? score.vol_of(lab[i]) : 0;
-    // a run's total is scored at its last element
+    // a run's total is scored at its last element.  Layered LP needs the
+    // label's volume there: loaded for run ends only, eight slots a round so
+    // that the loads of a round are in flight together without holding a
+    // register per slot
+    constexpr int U = TMAX < 8 ? TMAX : 8;
     Best best = best_none();
     uint32_t run = 0;
 #pragma unroll
-    for (int i = 0; i < TMAX; ++i) {
-      run = (i > 0 && lab[i] == lab[i > 0 ? i - 1 : 0]) ? run + wt[i] : wt[i];
-      const bool end = (i == TMAX - 1) || lab[(i + 1) & (TMAX - 1)] != lab[i];
-      if (end && lab[i] != INT32_MAX) {
-        const Best c{score.from_vol(run, vl[i]), lab[i]};
-        if (better(c, best)) best = c;
+    for (int i0 = 0; i0 < TMAX; i0 += U) {
+      int32_t vl[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + u;
+        const bool end = (i == TMAX - 1) || lab[(i + 1) & (TMAX - 1)] != lab[i];
+        vl[u] = (S::kScan && end && lab[i] != INT32_MAX) ? score.vol_of(lab[i]) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + u;
+        run = (i > 0 && lab[i] == lab[i > 0 ? i - 1 : 0]) ? run + wt[i] : wt[i];
+        const bool end = (i == TMAX - 1) || lab[(i + 1) & (TMAX - 1)] != lab[i];
+        if (end && lab[i] != INT32_MAX) {
+          const Best c{score.from_vol(run, vl[u]), lab[i]};
+          if (better(c, best)) best = c;
+        }
       }
     }
     a.lout[v] = best.l;
