@@ -85,7 +85,9 @@ typedef struct glp_params {
   /* degree tiers (0 = engine default / autotuned) */
   int32_t tiny_max;               /* thread per vertex up to this degree (<= 8) */
   int32_t mid_max;                /* warp per vertex up to this degree (32..256) */
-  int32_t big_max;                /* block per vertex up to this degree (mid_max..8192); above: hubs */
+  int32_t big_max;                /* block per vertex up to this degree (mid_max..24576 unweighted,
+                                     mid_max..8192 weighted); above: hubs.  0 = the largest the
+                                     graph allows (24576 unweighted, 8192 weighted) */
   int32_t hub_chunk;              /* edges per hub streaming block (256..65536) */
   int32_t use_graph;              /* capture the iteration loop in a CUDA graph */
   int32_t async;                  /* 1: enqueue on the stream and return without
@@ -150,7 +152,8 @@ int glp_graph_info(const glp_graph* g, int32_t* n, int64_t* m, int32_t* max_degr
  * out[15]: hub streaming chunks.  Mirrors the bin report of
  * prop/classicLprop.cuh:213-227. */
 int glp_graph_plan(glp_graph* g, const glp_params* p, int64_t out[16]);
-/* The same plan computed from host offsets alone (no device needed). */
+/* The same plan computed from host offsets alone (no device needed),
+ * planned as for an unweighted graph. */
 int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int64_t out[16]);
 /* Reports (and clears) kernel error flags raised by asynchronous runs. */
 int glp_graph_check(glp_graph* g);
