@@ -394,11 +394,12 @@ static bool serial_step() {
 template <bool W, class S>
 static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWork& tw, const S& score,
                            cudaStream_t s, int64_t* launches) {
-  const unsigned grid = (unsigned)std::min<int64_t>(p.big.n, 148 * 2);
+  const unsigned grid = (unsigned)std::min<int64_t>(p.big.n, 148 * 4);
   ++*launches;
   if constexpr (!W) {
-    if (p.big_part[kBigParts - 1].n) {
-      const size_t sm16 = (size_t)kBig16Slots * 6;
+    const bool top = p.big_part[kBigParts - 1].n > 0;
+    if (top || S::kPacked) {
+      const size_t sm16 = (size_t)(top ? kBig16Slots : 2 * kBigPartMax[kBigParts - 2]) * 6;
       GLP_CUDA(raise_smem_limit((const void*)k_big<512, false, S, true>, sm16));
       k_big<512, false, S, true><<<grid, 512, sm16, s>>>(a, tw, score);
       return GLP_OK;
@@ -507,13 +508,27 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     static_assert(kBigParts == 5 && kBigPartThreads[0] == 256 && kBigPartThreads[1] == 256 &&
                       kBigPartThreads[2] == 512 && kBigPartThreads[3] == 1024 && kBigPartThreads[4] == 1024,
                   "the launches below follow kBigPartThreads");
+    // unweighted classic counts fit 16 bits: from the second range on, the
+    // smaller 16-bit tables (and 32 registers a thread) fit twice the blocks
+    constexpr bool k16 = !W && S::kPacked;
     for (int r = 0; r < kBigParts; ++r) {
       const Verts& vs = p.big_part[r];
       if (!vs.n) continue;
       const TierWork tw{vs, none, none, 1};
       const size_t smr = 4ull * kBigPartMax[r] * sizeof(uint32_t);
       const unsigned grid = (unsigned)std::min<int64_t>(vs.n, kMaxGrid);
-      if (r < 2) {
+      if (k16 && r > 0 && r < kBigParts - 1) {
+        const size_t sm16 = 12ull * kBigPartMax[r];  // 2*max slots of 4 + 2 bytes
+        if (r == 1) {
+          k_big<256, false, S, true><<<grid, 256, sm16, s>>>(a, tw, score);
+        } else if (r == 2) {
+          if ((rc = allow_smem(k_big<512, false, S, true>, sm16))) return rc;
+          k_big<512, false, S, true><<<grid, 512, sm16, s>>>(a, tw, score);
+        } else {
+          if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
+          k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
+        }
+      } else if (r < 2) {
         k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
       } else if (r == 2) {
         if ((rc = allow_smem(k_big<512, W, S>, smr))) return rc;

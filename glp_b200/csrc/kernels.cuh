@@ -537,12 +537,12 @@ __device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32
 // vertex to the power of two >= 2*degree.  C16 (unweighted counts only):
 // 16-bit counts, and at most kBig16Slots slots (three quarters full at
 // degree 24576), so 24576 labels fit 192 KB of shared memory.
-// Classic blocks of up to 512 threads are held to 32 registers unweighted
-// (2048 threads per SM) and 42 weighted (1536), which they fit without
-// spilling; the other instantiations to 64 (1024 threads per SM).
+// Unweighted classic blocks are held to 32 registers (2048 threads per SM),
+// weighted classic blocks of up to 512 threads to 42 (1536), which they fit
+// without spilling; the other instantiations to 64 (1024 threads per SM).
 constexpr uint32_t kBig16Slots = 32768;
 template <int NT, bool W, class S, bool C16 = false>
-__global__ void __launch_bounds__(NT, (S::kPacked && !C16 && NT <= 512) ? (W ? 1536 : 2048) / NT : 1024 / NT) k_big(StepArgs a, TierWork tw, S score) {
+__global__ void __launch_bounds__(NT, (S::kPacked && !W) ? 2048 / NT : (S::kPacked && NT <= 512) ? 1536 / NT : 1024 / NT) k_big(StepArgs a, TierWork tw, S score) {
   static_assert(!(C16 && W), "16-bit counts hold unweighted counts only");
   const bool scan = S::kScan && scan_scores(a);
   extern __shared__ __align__(16) uint32_t smem[];
