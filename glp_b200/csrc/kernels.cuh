@@ -463,11 +463,15 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
 // sized to the power of two >= 2*degree; batches of 4 chunks of 32 edges are
 // loaded before they are counted.
 template <int CAP, int NT, bool W, class S>
-__global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
+__global__ void __launch_bounds__(NT, (S::kPacked && !W) ? 2048 / NT : (S::kPacked ? 1536 : 1024) / NT)
+    k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
+  // unweighted classic: 16-bit counts (a count never exceeds the degree),
+  // so the tables and 32 registers a thread fit eight blocks per SM
+  constexpr bool C16 = S::kPacked && !W;
   const bool scan = S::kScan && scan_scores(a);
   __shared__ __align__(16) uint32_t skeys[NW][CAP];
-  __shared__ __align__(16) uint32_t svals[NW][CAP];
+  __shared__ __align__(16) uint32_t svals[NW][C16 ? CAP / 2 : CAP];
   __shared__ int32_t cbuf[NW][32];  // changed vertices not yet listed
   uint32_t ncb = 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -480,12 +484,12 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
     const int32_t b = a.off[v], e = a.off[v + 1];
     const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));  // degree > 32: cap >= 128
     zero_words16(kk, cap, lane, 32);
-    zero_words16(vv, cap, lane, 32);
+    zero_words16(vv, C16 ? cap / 2 : cap, lane, 32);
     __syncwarp();
     Best best = best_none();
     bool fail = false;
     auto ins = [&](uint32_t key, uint32_t k) {
-      return table_insert_bounded(kk, vv, cap - 1, key, k, cap, nullptr, nullptr);
+      return table_insert_bounded<C16>(kk, vv, cap - 1, key, k, cap, nullptr, nullptr);
     };
     for (int32_t j0 = b; j0 < e; j0 += 128) {
       int32_t lab[4];
@@ -506,7 +510,7 @@ __global__ void __launch_bounds__(NT) k_mid(StepArgs a, TierWork tw, S score) {
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {
       __syncwarp();
-      scan_table(kk, vv, cap, lane, 32, score, best);
+      scan_table<C16>(kk, vv, cap, lane, 32, score, best);
     }
     best = group_max<32>(best);
     bool chg = false;
