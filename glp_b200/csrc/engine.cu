@@ -389,8 +389,9 @@ static bool serial_step() {
 
 // One launch over a device-built list of big-tier vertices (majority
 // failures, frontier members, screen fallbacks): 512-thread blocks with a
-// table for the tier's largest degree (16-bit counts when the tier reaches
-// past kBigMaxWeighted).
+// table for the tier's largest degree, with 16-bit counts on unweighted
+// graphs when the tier reaches past kBigMaxWeighted or the score is classic
+// (smaller tables, more blocks per SM).
 template <bool W, class S>
 static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWork& tw, const S& score,
                            cudaStream_t s, int64_t* launches) {
