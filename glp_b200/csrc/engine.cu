@@ -770,13 +770,46 @@ static int ensure_sorted(glp_graph* g) {
 }
 
 // Exact first step when the labels are the vertex ids and rows are strictly
-// ascending (k_first_step), timed as a step.
+// ascending: unweighted, the row's last column (k_first_step); weighted, the
+// row's largest (weight, label), per tier: a thread per vertex up to degree
+// 32, a warp per mid vertex, a block per big vertex and hub.
+template <bool W>
+static int launch_first_step(const DevicePlan& p, const StepArgs& a, cudaStream_t s, int64_t* launches) {
+  const unsigned kMaxGrid = 148 * 32;
+  if constexpr (!W) {
+    k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), kMaxGrid), 256, 0, s>>>(a);
+    ++*launches;
+  } else {
+    for (const Verts* vs : {&p.tiny, &p.g16, &p.g32})
+      if (vs->n) {
+        k_first_step_w<1><<<(unsigned)std::min<int64_t>(cdiv(vs->n, 256), kMaxGrid), 256, 0, s>>>(a, *vs);
+        ++*launches;
+      }
+    if (p.mid.n) {
+      k_first_step_w<32><<<(unsigned)std::min<int64_t>(cdiv((int64_t)p.mid.n * 32, 256), kMaxGrid), 256, 0, s>>>(
+          a, p.mid);
+      ++*launches;
+    }
+    if (p.big.n) {
+      k_first_step_w_block<256><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), 256, 0, s>>>(a, p.big);
+      ++*launches;
+    }
+    if (p.n_hubs) {
+      k_first_step_w_block<1024><<<(unsigned)p.n_hubs, 1024, 0, s>>>(a, Verts{p.hub.hub_v, 0, p.n_hubs});
+      ++*launches;
+    }
+  }
+  GLP_CUDA(cudaGetLastError());
+  return GLP_OK;
+}
+
+// The first step as its own timed step.
+template <bool W>
 static int first_step(RunCtx& c, const StepArgs& a) {
   StepLaunch L = c.launch();
   if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[16], c.s));
-  k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), 148 * 32), 256, 0, c.s>>>(a);
-  ++c.launches;
-  GLP_CUDA(cudaGetLastError());
+  int rc = launch_first_step<W>(c.g->plan, a, c.s, &c.launches);
+  if (rc) return rc;
   if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[17], c.s));
   return GLP_OK;
 }
@@ -823,12 +856,12 @@ static int run_classic(RunCtx& c, int32_t niter) {
       L.front.chg_in = p.chg[(it - 1) & 1];
       L.front.chg_in_n = p.counts + 7 + ((it - 1) & 1);
     }
-    if (it == 0 && !W && g->rows_sorted == 1) {
+    if (it == 0 && g->rows_sorted == 1) {
       if (c.timing) {  // first_step takes the step's events itself
         c.used--;
         c.ran.pop_back();
       }
-      if ((rc = first_step(c, a))) return rc;
+      if ((rc = first_step<W>(c, a))) return rc;
     } else if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) {
       return rc;
     }
@@ -907,12 +940,10 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
                g->plan.d_mode, g->n, nullptr, nullptr};
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
     L.allow_majority = 1;  // the listener mode; spoken labels change every step: no frontier
-    if (it == 0 && !W && g->rows_sorted == 1) {
+    if (it == 0 && g->rows_sorted == 1) {
       // the step's events were taken by c.launch() above; the first step records them
       if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[16], c.s));
-      k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), 148 * 32), 256, 0, c.s>>>(a);
-      ++c.launches;
-      GLP_CUDA(cudaGetLastError());
+      if ((rc = launch_first_step<W>(g->plan, a, c.s, &c.launches))) return rc;
       if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[17], c.s));
     } else if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) {
       return rc;

@@ -960,6 +960,59 @@ __global__ void __launch_bounds__(256) k_first_step(StepArgs a) {
   }
 }
 
+// The weighted form of the same shortcut: every neighbour label occurs once,
+// so its count is the edge's weight, and the step takes the neighbour label
+// of largest (weight, label).  G lanes per vertex (1 or 32); the rows of the
+// big tier and the hubs go to k_first_step_w_block.
+__device__ __forceinline__ unsigned long long first_key_w(const StepArgs& a, int32_t j) {
+  return ((unsigned long long)(uint32_t)a.w[j] << 32) | (uint32_t)a.lin[a.cols[j]];
+}
+template <int G>
+__global__ void __launch_bounds__(256) k_first_step_w(StepArgs a, Verts vs) {
+  const int lane = threadIdx.x & (G - 1);
+  for (int64_t t0 = (int64_t)blockIdx.x * blockDim.x; t0 < (int64_t)vs.n * G; t0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = (t0 + threadIdx.x) / G;
+    bool chg = false;
+    int32_t v = 0;
+    unsigned long long best = 0ull;
+    if (i < vs.n) {
+      v = vs[i];
+      const int32_t b = a.off[v], e = a.off[v + 1];
+      for (int32_t j = b + lane; j < e; j += G) best = max(best, first_key_w(a, j));
+    }
+#pragma unroll
+    for (int m = G / 2; m >= 1; m >>= 1) best = max(best, __shfl_xor_sync(kFull, best, m));
+    if (i < vs.n && lane == 0 && a.off[v + 1] > a.off[v]) {
+      const int32_t l = (int32_t)(uint32_t)best;
+      a.lout[v] = l;
+      chg = l != a.lcur[v];
+    }
+    record_changes(a, chg, v);
+  }
+}
+template <int NT>
+__global__ void __launch_bounds__(NT) k_first_step_w_block(StepArgs a, Verts vs) {
+  __shared__ unsigned long long sb;
+  for (int32_t i = blockIdx.x; i < vs.n; i += gridDim.x) {
+    const int32_t v = vs[i];
+    const int32_t b = a.off[v], e = a.off[v + 1];
+    if (threadIdx.x == 0) sb = 0ull;
+    __syncthreads();
+    unsigned long long best = 0ull;
+    for (int32_t j = b + threadIdx.x; j < e; j += NT) best = max(best, first_key_w(a, j));
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) best = max(best, __shfl_xor_sync(kFull, best, m));
+    if ((threadIdx.x & 31) == 0) atomicMax(&sb, best);
+    __syncthreads();
+    if (threadIdx.x == 0 && e > b) {
+      const int32_t l = (int32_t)(uint32_t)sb;
+      a.lout[v] = l;
+      if (l != a.lcur[v]) record_change(a, v);
+    }
+    __syncthreads();  // sb is reset for the next vertex
+  }
+}
+
 // bad |= 1 when some row is not strictly ascending.  One warp per row, 8
 // column pairs in flight per lane.
 __global__ void __launch_bounds__(256) k_check_sorted(const int32_t* __restrict__ off,

@@ -146,6 +146,23 @@ def test_slpa_memory_sizes(T, niter):
     np.testing.assert_array_equal(res.slpa_comm, ref["comm"])
 
 
+@pytest.mark.parametrize("tier", ["default", "small_hubs"])
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_10000"])
+def test_slpa_weighted(case, tier):
+    """Weighted SLPA listener, including its first step (every spoken label
+    distinct: the neighbour of largest weight, then largest label, wins)."""
+    off, cols = CASES[case]
+    w = graphs.add_weights(from_numpy(off, cols), 16, seed=5).weights.numpy()
+    T, niter, seed, r = 8, 10, 4, 0.1
+    with Graph(from_numpy(off, cols, w)) as g:
+        res = g.run(_lib.METHOD_SLPA, niter, make_params(slpa_T=T, seed=seed, slpa_r=r, **TIERS[tier]),
+                    slpa_outputs=True)
+    ref = O.slpa_run(off, cols, T, niter, seed, r, w=w)
+    np.testing.assert_array_equal(res.labels, ref["labels"])
+    np.testing.assert_array_equal(res.slpa_mem, ref["mem"])
+    np.testing.assert_array_equal(res.slpa_comm, ref["comm"])
+
+
 @pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000"])
 def test_hooks_classic_equals_method1(case):
     off, cols = CASES[case]
