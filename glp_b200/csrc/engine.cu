@@ -253,6 +253,8 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
   DevicePlan& p = g->plan;
   p.tiers = t;
   p.setup = g->stream;
+  // weighted mid counts fit 16 bits when no mid vertex's weights sum past it
+  p.mid_c16 = g->d_w == nullptr || g->mid_wsum < 65536u;
   int rc;
   int64_t n_mid = 0, n_big = 0, ntier[5] = {0, 0, 0, 0, 0};
   if (g->deg_sorted == 1) {
@@ -554,8 +556,13 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   }
   if (p.mid.n) {
     if ((rc = mark_on(s, 3, 0))) return rc;
-    k_mid<kMidCap, kMidNT, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.mid.n, kMidNT / 32), kMaxGrid), kMidNT, 0, s>>>(
-        a, work(p.mid, 3, &p.fmid), score);
+    const unsigned grid = (unsigned)std::min<int64_t>(cdiv(p.mid.n, kMidNT / 32), kMaxGrid);
+    bool c16w = false;  // weighted classic with small weight sums: 16-bit counts
+    if constexpr (W && S::kPacked) {
+      c16w = p.mid_c16;
+      if (c16w) k_mid<kMidCap, kMidNT, W, S, true><<<grid, kMidNT, 0, s>>>(a, work(p.mid, 3, &p.fmid), score);
+    }
+    if (!c16w) k_mid<kMidCap, kMidNT, W, S><<<grid, kMidNT, 0, s>>>(a, work(p.mid, 3, &p.fmid), score);
     if ((rc = mark_on(s, 3, 1))) return rc;
     ++*launches;
   }
@@ -1000,20 +1007,31 @@ __global__ void k_validate_offsets(const int32_t* __restrict__ off, int32_t n, i
 
 // Columns in [0, n) (bad 1), weights >= 0 (bad 2), per-vertex weight sums
 // below 2^31 (bad 4).  Runs only on valid offsets.
+// mid_wsum: the largest weight sum of a vertex of degree <= kMidCap / 2 (a
+// bound on any of its label counts).
 __global__ void k_validate(const int32_t* __restrict__ off, const int32_t* __restrict__ cols,
-                           const int32_t* __restrict__ w, int64_t m, int32_t n, uint32_t* bad) {
+                           const int32_t* __restrict__ w, int64_t m, int32_t n, uint32_t* bad, uint32_t* mid_wsum) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
     const int32_t c = cols[j];
     if (c < 0 || c >= n) atomicOr(bad, 1u);
     if (w && w[j] < 0) atomicOr(bad, 2u);
   }
   // the engine sums a vertex's weights in 32 bits
-  if (w)
-    for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-      int64_t sum = 0;
-      for (int32_t j = off[v]; j < off[v + 1]; ++j) sum += w[j];
-      if (sum >= 2147483648LL) atomicOr(bad, 4u);
+  if (w) {
+    uint32_t mid_max = 0;
+    const int32_t nv = (n + 31) & ~31;  // whole warps for the reduction
+    for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+      if (v < n) {
+        int64_t sum = 0;
+        for (int32_t j = off[v]; j < off[v + 1]; ++j) sum += w[j];
+        if (sum >= 2147483648LL) atomicOr(bad, 4u);
+        if (off[v + 1] - off[v] <= kMidCap / 2 && sum > 0)
+          mid_max = max(mid_max, sum < 0xffffffffLL ? (uint32_t)sum : 0xffffffffu);
+      }
     }
+    mid_max = __reduce_max_sync(kFull, mid_max);
+    if ((threadIdx.x & 31) == 0 && mid_max) atomicMax(mid_wsum, mid_max);
+  }
 }
 
 int validate_csr_device(glp_graph* g) {
@@ -1021,6 +1039,7 @@ int validate_csr_device(glp_graph* g) {
     uint32_t bad;
     int32_t maxdeg;
     uint32_t unsorted;
+    uint32_t mid_wsum;
   };
   Flags* d_f = nullptr;
   GLP_CUDA(dev_alloc(&d_f, sizeof(Flags)));
@@ -1029,8 +1048,8 @@ int validate_csr_device(glp_graph* g) {
   Flags f{};
   cudaError_t e = cudaMemcpy(&f, d_f, sizeof f, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && !f.bad && g->m) {
-    k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, &d_f->bad);
-    e = cudaMemcpy(&f.bad, &d_f->bad, sizeof f.bad, cudaMemcpyDeviceToHost);
+    k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, &d_f->bad, &d_f->mid_wsum);
+    e = cudaMemcpy(&f, d_f, sizeof f, cudaMemcpyDeviceToHost);
   }
   dev_free(d_f);
   if (e != cudaSuccess) return cuda_fail(e, "validate");
@@ -1056,6 +1075,7 @@ int validate_csr_device(glp_graph* g) {
   }
   g->max_degree = f.maxdeg;
   g->deg_sorted = f.unsorted ? 0 : 1;
+  g->mid_wsum = f.mid_wsum;
   return GLP_OK;
 }
 
@@ -1691,7 +1711,7 @@ int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int
     return GLP_OK;
   }
   k_validate_offsets<<<1184, 256, 0, st>>>(d_offsets, n, m, &sc->bad, &sc->maxdeg, &sc->unsorted);
-  if (m) k_validate<<<1184, 256, 0, st>>>(d_offsets, d_cols, nullptr, m, n, &sc->bad);
+  if (m) k_validate<<<1184, 256, 0, st>>>(d_offsets, d_cols, nullptr, m, n, &sc->bad, nullptr);
   GLP_CUDA(cudaGetLastError());
   uint32_t flags[2] = {0, 0};  // bad, maxdeg
   GLP_CUDA(cudaMemcpyAsync(flags, &sc->bad, sizeof flags, cudaMemcpyDeviceToHost, st));

@@ -80,6 +80,7 @@ struct DevicePlan {
   int32_t* chg[2] = {nullptr, nullptr};
   Frontier front{};
   int32_t* d_mode = nullptr;
+  bool mid_c16 = true;  // mid counts fit 16 bits (unweighted, or small weight sums)
   int32_t n_hubs = 0, n_chunks = 0;
   int64_t isolated = 0;
   HubPlan hub{};
@@ -134,6 +135,7 @@ struct glp_graph {
   int symmetric = -1;    // -1 unknown, 0 no, 1 yes (every edge stored both ways)
   int rows_sorted = -1;  // -1 unknown, 0 no, 1 every row strictly ascending
   int deg_sorted = 0;    // 1: degrees never increase along the vertex ids
+  uint32_t mid_wsum = 0;  // weighted: largest weight sum of a vertex of degree <= kMidCap / 2
   cudaStream_t last_stream = nullptr;  // the stream of the latest run
   uint32_t epoch = 0;  // frontier mark of the last step
   // auxiliary streams and fork/join events of a step

@@ -462,13 +462,13 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
 // Exact count, one warp per vertex (degree <= CAP/2): per-warp shared table
 // sized to the power of two >= 2*degree; batches of 4 chunks of 32 edges are
 // loaded before they are counted.
-template <int CAP, int NT, bool W, class S>
-__global__ void __launch_bounds__(NT, (S::kPacked && !W) ? 2048 / NT : (S::kPacked ? 1536 : 1024) / NT)
+// C16: 16-bit counts (unweighted: a count never exceeds the degree;
+// weighted: the caller knows every mid vertex's weights sum below 2^16), so
+// that the tables and 32 registers a thread fit eight blocks per SM.
+template <int CAP, int NT, bool W, class S, bool C16 = (S::kPacked && !W)>
+__global__ void __launch_bounds__(NT, S::kPacked ? (C16 ? 2048 : 1536) / NT : 1024 / NT)
     k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
-  // unweighted classic: 16-bit counts (a count never exceeds the degree),
-  // so the tables and 32 registers a thread fit eight blocks per SM
-  constexpr bool C16 = S::kPacked && !W;
   const bool scan = S::kScan && scan_scores(a);
   __shared__ __align__(16) uint32_t skeys[NW][CAP];
   __shared__ __align__(16) uint32_t svals[NW][C16 ? CAP / 2 : CAP];

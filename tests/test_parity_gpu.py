@@ -92,6 +92,20 @@ def test_weighted_per_iteration(case, tier):
         np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
 
 
+@pytest.mark.parametrize("case", ["rmat12", "planted20k"])
+def test_weighted_large_weights(case):
+    """Weights large enough that mid-tier weight sums pass 2^16: the mid tier
+    keeps 32-bit counts (small weights use 16-bit ones)."""
+    off, cols = CASES[case]
+    w = graphs.add_weights(from_numpy(off, cols), 1_000_000, seed=11).weights.numpy()
+    assert int(np.diff(off).max()) * 1_000_000 < 2 ** 31
+    niter = 6
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, niter, w=w)
+    _, otr = O.classic_run(off, cols, niter, w=w, trace=True)
+    for it in range(niter):
+        np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
+
+
 @pytest.mark.parametrize("tier", ["default", "small_hubs", "mostly_hubs"])
 @pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "star_ring_10000", "two_cliques",
                                   "planted20k"])
