@@ -207,10 +207,13 @@ def profiled_traffic():
 # ----------------------------------------------------------------- workload
 def make_graph(scale: int, seed: int, device):
     from glp_b200 import graphs
-    torch.cuda.synchronize()
+    on_gpu = torch.device(device).type == "cuda"
+    if on_gpu:
+        torch.cuda.synchronize()
     t0 = time.perf_counter()
     g = graphs.rmat(scale, 16, seed=seed, device=device)
-    torch.cuda.synchronize()
+    if on_gpu:
+        torch.cuda.synchronize()
     return g, time.perf_counter() - t0
 
 
@@ -249,11 +252,14 @@ def run_reference(args, ws, rank):
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_cpulp")):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_cpulp was not built"}))
         return
-    g, _ = make_graph(args.scale, args.seed, "cuda")
+    # the samplers give the same graph on the host and the device; the device
+    # is only faster at generating it
+    g, _ = make_graph(args.scale, args.seed, "cuda" if torch.cuda.is_available() else "cpu")
     off, cols, _ = g.numpy()
     n, m = len(off) - 1, len(cols)
     del g
-    torch.cuda.empty_cache()
+    if torch.cuda.is_available():
+        torch.cuda.empty_cache()
     # a reference step is one CPU iteration of the full graph (about 30 s at
     # scale 24 on 16 cores), so the run is bounded to 1 warm-up + 4 timed
     # iterations whatever --steps / --warmup ask: the metric is per iteration

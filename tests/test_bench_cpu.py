@@ -1,0 +1,32 @@
+"""The reference arm of bench.py -- the reference's own CPU path
+(tutorial/CPUlp.cuh, built from source into oracle/_ref) timed on the host --
+prints one JSON line of the bench contract.  It needs no GPU, so it is
+checked here at a small scale."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_one_contract_line():
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--scale", "10", "--steps", "2",
+                        "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference"
+    if "unavailable" in line:  # the reference binary was not built in this tree
+        assert not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_cpulp"))
+        return
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["value"] > 0 and line["unit"] == "GTEPS" and line["higher_is_better"] is True
+    assert line["steps"] == 2 and line["warmup"] == 1
+    assert line["config"]["n"] == 1024 and line["config"]["workload"] == "rmat10-ef16-seed2-classic-20it"
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
