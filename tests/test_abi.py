@@ -104,3 +104,16 @@ def test_bad_method_and_null_args():
     rc = lib.glp_run(None, 1, None, 1, C.byref(out), _lib.ITER_CB(), None, None)
     assert rc == _lib.GLP_EINVAL
     assert b"required" in lib.glp_last_error()
+
+
+def test_summary_entry_points_reject_null_args():
+    lib = _lib.load()
+    rows = (C.c_uint32 * 24)()
+    verts = (C.c_int32 * 1)(0)
+    labels = (C.c_int32 * 1)(0)
+    rc = lib.glp_graph_cm_sketch(None, labels, 0, verts, 1, 8, 0, rows)
+    assert rc == _lib.GLP_EINVAL and b"required" in lib.glp_last_error()
+    keys, vals = (C.c_uint32 * 8)(), (C.c_uint32 * 8)()
+    rounds = (C.c_int32 * 1)()
+    rc = lib.glp_graph_fa_summary(None, labels, 0, verts, 1, 8, 0, keys, vals, rounds)
+    assert rc == _lib.GLP_EINVAL and b"required" in lib.glp_last_error()
