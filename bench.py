@@ -13,19 +13,26 @@ the device-resident graph.  GTEPS = CSR entries x iterations / seconds.
 * e2e: the same metric through the public API with host buffers: every step
   copies the CSR from pinned host memory (glp_graph_create), runs, and reads
   the labels back into a pinned host buffer.
-* roofline: the dominant kernel tier, algorithmic bytes 8*m_t + 12*n_t per
-  launch over its CUDA-event launch time, against the measured HBM copy peak.
-  Tier times come from PROFILE_RUNS further runs after the timed region, with
-  the step's kernels on one stream so that each tier's events bracket only
-  its own kernels (the timed runs overlap tiers on three streams).
+* roofline: the dominant kernel group in the steps that count every vertex
+  of the group (full-count steps; the other steps recount only majority
+  failures or the neighbours of changed vertices), algorithmic bytes
+  8*m_t + 12*n_t per launch over its CUDA-event launch time, against the
+  measured HBM copy peak.  Tier times come from PROFILE_RUNS further runs
+  after the timed region, with the step's kernels on one stream so that each
+  tier's events bracket only its own kernels (the timed runs overlap tiers on
+  three streams).  whole_step_roofline: 8m + 12n + 4 bytes per iteration over
+  the mean iteration time of the timed runs.
 * cpu_baseline: the reference's own OpenMP CPU path (tutorial/CPUlp.cuh,
-  compiled from source into oracle/_ref) on the same graph, one iteration.
+  compiled from source into oracle/_ref) on the same graph: all iterations of
+  one run from label = id, the same run --impl reference times.
+* parity: the headline run's final labels against the CPU oracle.
 
 Multi-GPU: each rank runs an independent replica (the path does not shard
 across GPUs); value = total edges*iterations of all ranks / max rank time.
 
 --impl reference times the reference's own CPU implementation instead
-(rank 0 only), one LP iteration per step on the same graph.
+(rank 0 only): one step = one LP iteration, the steps being the iterations of
+one run on the same graph, which it builds on the host without the engine.
 """
 from __future__ import annotations
 
@@ -63,7 +70,6 @@ def parse():
     ap.add_argument("--iters", type=int, default=ITERS)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-iters", type=int, default=1)
     ap.add_argument("--workload", default="classic", choices=["classic", "batched", "served"],
                     help="classic: the R-MAT headline line (with a batched summary unless --no-batched); "
                          "batched: the batched workload alone")
@@ -217,6 +223,13 @@ def make_graph(scale: int, seed: int, device):
     return g, time.perf_counter() - t0
 
 
+def workload_config(args, n: int, m: int) -> dict:
+    """The workload's config object, identical in both arms."""
+    return {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic-{args.iters}it", "n": int(n), "m": int(m),
+            "iterations_per_run": args.iters,
+            "l2": "inputs larger than L2 (CSR %.2f GB); no flush" % ((4 * (n + 1 + m)) / 1e9)}
+
+
 def write_csr(path: str, off: np.ndarray, cols: np.ndarray):
     with open(path, "wb") as f:
         np.array([len(off) - 1, len(cols)], dtype=np.int64).tofile(f)
@@ -224,70 +237,125 @@ def write_csr(path: str, off: np.ndarray, cols: np.ndarray):
         cols.astype(np.int32).tofile(f)
 
 
-def ref_cpulp_run(csr_path: str, niter: int, threads: int | None = None):
-    """Run the reference CPUlp::sync_run_1 (oracle/_ref/ref_cpulp) and return
-    its per-iteration seconds as printed by the reference."""
+def cpu_threads() -> int:
+    """Threads of the reference CPU path: CPUlp.cuh:50 hard-codes
+    num_threads(20); OMP_THREAD_LIMIT caps it at the host's CPUs so that it is
+    not oversubscribed (it cannot use more than 20 without editing it)."""
+    return max(1, min(20, os.cpu_count() or 1))
+
+
+def ref_cpulp_run(csr_path: str, niter: int, threads: int):
+    """Run the reference CPUlp::sync_run_1 (oracle/_ref/ref_cpulp) for niter
+    iterations from label = id; returns (per-iteration seconds as printed by
+    the reference, final labels)."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_cpulp")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     env = dict(os.environ)
-    if threads:
-        env["OMP_THREAD_LIMIT"] = str(threads)
+    env["OMP_THREAD_LIMIT"] = str(threads)
     with tempfile.TemporaryDirectory() as d:
-        r = subprocess.run([exe, "sync-csr", csr_path, str(niter), os.path.join(d, "l.bin")], capture_output=True,
-                           text=True, env=env, check=True)
-    return [float(x) for x in re.findall(r"t1: ([0-9.eE+-]+)", r.stdout)]
+        out = os.path.join(d, "l.bin")
+        r = subprocess.run([exe, "sync-csr", csr_path, str(niter), out], capture_output=True, text=True, env=env,
+                           check=True)
+        labels = np.fromfile(out, dtype=np.int32)
+    return [float(x) for x in re.findall(r"t1: ([0-9.eE+-]+)", r.stdout)], labels
 
 
-def cpu_threads_used() -> int:
-    # CPUlp.cuh:50 hard-codes num_threads(20); the OpenMP runtime may cap it
-    lim = os.environ.get("OMP_THREAD_LIMIT")
-    return min(20, int(lim)) if lim else 20
+def cpu_reference_leg(args, off: np.ndarray, cols: np.ndarray, niter: int) -> dict:
+    """The reference's own OpenMP CPU path (tutorial/CPUlp.cuh sync_run_1,
+    compiled from source into oracle/_ref) on the workload graph: one run of
+    niter iterations from label = id, iteration 0 included, timed by the
+    reference's own per-iteration timer."""
+    n, m = len(off) - 1, len(cols)
+    threads = cpu_threads()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "g.csr")
+        write_csr(path, off, cols)
+        times, _ = ref_cpulp_run(path, niter, threads)
+    t = sum(times)
+    return {"value": round(m * len(times) / t / 1e9, 4), "unit": "GTEPS", "cores": threads, "kind": "reference",
+            "iterations": len(times), "seconds": round(t, 2), "host_cpus": os.cpu_count(),
+            "sample": f"reference CPUlp::sync_run_1 (tutorial/CPUlp.cuh, built from source), all {len(times)} "
+                      f"iterations of one run from label = id on the full graph (n={n}, m={m}), {t:.1f} s; "
+                      f"OMP_THREAD_LIMIT={threads} on a host with {os.cpu_count()} cpus"}
 
 
 # ----------------------------------------------------------------- arms
 def run_reference(args, ws, rank):
+    """The reference's own CPU implementation of the path (no engine code: the
+    graph is built on the host by the oracle's restatement of the sampler)."""
     if rank != 0:
         return
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_cpulp")):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_cpulp was not built"}))
         return
-    # the samplers give the same graph on the host and the device; the device
-    # is only faster at generating it
-    g, _ = make_graph(args.scale, args.seed, "cuda" if torch.cuda.is_available() else "cpu")
-    off, cols, _ = g.numpy()
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    off, cols = O.rmat_csr(args.scale, 16, seed=args.seed)
+    gen_s = time.perf_counter() - t0
     n, m = len(off) - 1, len(cols)
-    del g
-    if torch.cuda.is_available():
-        torch.cuda.empty_cache()
-    # a reference step is one CPU iteration of the full graph (about 30 s at
-    # scale 24 on 16 cores), so the run is bounded to 1 warm-up + 4 timed
-    # iterations whatever --steps / --warmup ask: the metric is per iteration
-    warm, steps = min(args.warmup, 1), max(1, min(args.steps, 4))
-    with tempfile.TemporaryDirectory() as d:
-        path = os.path.join(d, "g.csr")
-        write_csr(path, off, cols)
-        times = ref_cpulp_run(path, warm + steps)
-    timed = times[warm:]
-    t = sum(timed)
-    value = m * len(timed) / t / 1e9
-    cores = cpu_threads_used()
-    sample = (f"CPUlp::sync_run_1 on the full R-MAT s{args.scale} graph (n={n}, m={m}); steps = reference LP "
-              f"iterations {warm}..{warm + steps - 1} after {warm} warm-up iteration(s), bounded from "
-              f"--steps {args.steps} --warmup {args.warmup}")
+    # one step = one CPU iteration; the steps are the first --steps iterations
+    # (at most the workload's own count) of one run, iteration 0 included
+    leg = cpu_reference_leg(args, off, cols, max(1, min(args.steps, args.iters)))
+    steps = leg["iterations"]
+    t = leg["seconds"]
     line = {
-        "metric": f"classic LP GTEPS per iteration, R-MAT scale {args.scale}", "value": round(value, 4),
-        "unit": "GTEPS", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
-        "ms_per_step": round(1000 * t / len(timed), 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the box",
-        "config": {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic-{args.iters}it", "n": n, "m": m,
-                   "step": "one reference CPU iteration"},
+        "metric": f"classic LP GTEPS per iteration, R-MAT scale {args.scale}", "value": leg["value"],
+        "unit": "GTEPS", "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+        "ms_per_step": round(1000 * t / max(steps, 1), 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the host",
+        "config": workload_config(args, n, m),
+        "step": "one reference CPU iteration; the steps are iterations 0..%d of one run from label = id "
+                "(a CPU iteration needs no warm-up, so --warmup %d is not applied)" % (steps - 1, args.warmup),
+        "graph_gen_s": round(gen_s, 2),
         "impl": "reference",
-        "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
-                         "sample": sample},
-        "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {k: leg[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": leg["value"], "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def full_count_roofline(plan: dict, runs: list, n: int, peak: float) -> dict:
+    """Roofline of the dominant kernel group over the steps that count every
+    vertex of the group.  A classic step after the first runs in full mode
+    unless the previous step changed fewer than n/4 labels (then only the
+    vertices that fail a majority test, or below n/20 only the neighbours of
+    changed vertices, are recounted); the first step of a graph with ascending
+    rows is a closed form and launches no tier kernel.  Bytes per launch are
+    the group's algorithmic bytes, 8 per CSR entry (column + neighbour label)
+    and 12 per vertex (offsets, own label, written label)."""
+    per = {}
+    full_steps = 0
+    for r in runs:
+        ch = r.changed
+        st = r.extra.get("step_tier_ms") if r.extra else None
+        if st is None:
+            continue
+        for it in range(1, len(ch)):
+            if ch[it - 1] * 4 < n:
+                continue
+            full_steps += 1
+            for t, key in TIER_PLAN_KEYS.items():
+                per.setdefault(key, 0.0)
+                per[key] += float(st[it][t])
+    if not per or full_steps == 0:
+        return {}
+    key = max(per, key=per.get)
+    n_t, m_t = plan[f"v_{key}"], plan[f"e_{key}"]
+    bytes_launch = 8 * m_t + 12 * n_t
+    avg_ms = per[key] / full_steps
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    groups = {}
+    for k, ms in per.items():
+        if ms <= 0:
+            continue
+        b = 8 * plan[f"e_{k}"] + 12 * plan[f"v_{k}"]
+        a = b / (ms / full_steps / 1e3) / 1e9
+        groups[k] = {"avg_ms": round(ms / full_steps, 4), "bytes_per_launch": int(b), "achieved_gbs": round(a, 1),
+                     "frac": round(a / peak, 4)}
+    return {"kernel": f"k_{key}", "bytes_per_launch": int(bytes_launch), "avg_launch_ms": round(avg_ms, 4),
+            "achieved": round(achieved, 1), "frac": round(achieved / peak, 4), "full_count_launches": full_steps,
+            "groups": groups}
 
 
 def run_glp(args, ws, rank, local):
@@ -327,16 +395,15 @@ def run_glp(args, ws, rank, local):
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     # per-tier kernel times, outside the timed region: the same run with every
-    # kernel of a step on one stream (GLP_SERIAL_STEP=1), so that a tier's
-    # CUDA-event time is its kernels' own duration, not a span shared with
-    # the tiers running beside it
-    os.environ["GLP_SERIAL_STEP"] = "1"
-    try:
-        for _ in range(PROFILE_RUNS):
-            r = handle.run(_lib.METHOD_CLASSIC, args.iters, params, labels_out=labels_dev, stream=sp, profile=True)
-            tier_ms += r.tier_ms
-    finally:
-        os.environ.pop("GLP_SERIAL_STEP", None)
+    # kernel of a step on one stream (serial_step), so that a tier's CUDA-event
+    # time is its kernels' own duration, not a span shared with the tiers
+    # running beside it
+    prof_params = make_params(serial_step=1)
+    prof_runs = []
+    for _ in range(PROFILE_RUNS):
+        r = handle.run(_lib.METHOD_CLASSIC, args.iters, prof_params, labels_out=labels_dev, stream=sp, profile=True)
+        tier_ms += r.tier_ms
+        prof_runs.append(r)
     torch.cuda.synchronize(dev)
     ms_max = max_over_ranks(ws, ms)
     edges_total = sum_over_ranks(ws, float(m) * args.iters * args.steps)
@@ -365,37 +432,39 @@ def run_glp(args, ws, rank, local):
     e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
     e2e_edges = sum_over_ranks(ws, float(m) * args.iters * args.e2e_steps)
     e2e_value = e2e_edges / (e2e_ms / 1e3) / 1e9
-    same = bool(np.array_equal(lab_pin.numpy(), labels_dev.cpu().numpy()))
+    dev_labels = labels_dev.cpu().numpy()
+    same = bool(np.array_equal(lab_pin.numpy(), dev_labels))
 
-    # roofline of the dominant kernel tier
+    # roofline of the dominant kernel group, over the steps that count every
+    # vertex of the group (full-count steps)
     peak, peak_kind = measured_peak()
     launches_per_tier = PROFILE_RUNS * args.iters
-    dom = max(TIER_PLAN_KEYS, key=lambda i: tier_ms[i])
-    key = TIER_PLAN_KEYS[dom]
-    n_t, m_t = plan[f"v_{key}"], plan[f"e_{key}"]  # vertices and CSR entries of that kernel group
-    bytes_launch = 8 * m_t + 12 * n_t
-    avg_ms = tier_ms[dom] / launches_per_tier
-    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
-    traffic = profiled_traffic().get(key)
+    roof = full_count_roofline(plan, prof_runs, n, peak)
+    key = roof["kernel"][2:] if roof else "big"
+    traffic = profiled_traffic().get("full_count_launch", {}).get(key)
     total_bytes_iter = 8 * m + 12 * n + 4
     iter_ms = ms / (args.steps * args.iters)
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        off_np, cols_np = off_h.numpy(), cols_h.numpy()
         try:
-            off_np, cols_np = off_h.numpy(), cols_h.numpy()
-            with tempfile.TemporaryDirectory() as d:
-                path = os.path.join(d, "g.csr")
-                write_csr(path, off_np, cols_np)
-                times = ref_cpulp_run(path, args.cpu_iters)
-            tcpu = sum(times)
-            cpu = {"value": round(m * len(times) / tcpu / 1e9, 4), "unit": "GTEPS", "cores": cpu_threads_used(),
-                   "kind": "reference",
-                   "sample": f"reference CPUlp::sync_run_1 (tutorial/CPUlp.cuh, built from source), "
-                             f"{len(times)} iteration(s) on the full graph, {tcpu:.2f} s; host has "
-                             f"{os.cpu_count()} cpus"}
+            cpu = cpu_reference_leg(args, off_np, cols_np, args.iters)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GTEPS", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+        # parity of the headline run's final labels with the oracle (the
+        # synchronous rule restated on the CPU), outside every timed region
+        try:
+            from oracle import oracle as O
+            t0 = time.perf_counter()
+            ref = O.classic_run(off_np, cols_np, args.iters)
+            parity = {"labels_equal_oracle": bool(np.array_equal(ref, dev_labels)),
+                      "mismatches": int(np.count_nonzero(ref != dev_labels)),
+                      "oracle_s": round(time.perf_counter() - t0, 1),
+                      "what": f"final labels after {args.iters} iterations vs the CPU oracle's synchronous rule"}
+        except Exception as e:
+            parity = {"labels_equal_oracle": None, "what": f"oracle failed: {e}"}
 
     if rank == 0:
         line = {
@@ -403,17 +472,20 @@ def run_glp(args, ws, rank, local):
             "value": round(value, 3), "unit": "GTEPS", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the GPU",
-            "config": {"workload": f"rmat{args.scale}-ef16-seed{args.seed}-classic-{args.iters}it", "n": n, "m": m,
-                       "iterations_per_step": args.iters, "parallelism": f"replicas{ws}",
-                       "l2": "inputs larger than L2 (CSR %.2f GB); no flush" % ((4 * (n + 1 + m)) / 1e9),
-                       "graph_gen_s": round(gen_s, 2)},
+            "config": workload_config(args, n, m),
+            "step": f"one {args.iters}-iteration run over the device-resident graph",
+            "parallelism": f"replicas{ws}", "graph_gen_s": round(gen_s, 2),
             "e2e": {"value": round(e2e_value, 3), "unit": "GTEPS", "h2d_bytes_per_step": int(4 * (n + 1 + m)),
                     "d2h_bytes_per_step": int(4 * n), "steps": args.e2e_steps, "labels_match_device_run": same},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": f"k_{key}",
-                         "peak_kind": peak_kind, "bytes_per_launch": int(bytes_launch),
-                         "avg_launch_ms": round(avg_ms, 4)},
+            "roofline": {"bound": "hbm", "achieved": roof.get("achieved"), "peak": peak, "unit": "GB/s",
+                         "frac": roof.get("frac"), "traffic": traffic, "kernel": roof.get("kernel"),
+                         "peak_kind": peak_kind, "bytes_per_launch": roof.get("bytes_per_launch"),
+                         "avg_launch_ms": roof.get("avg_launch_ms"),
+                         "launches": roof.get("full_count_launches"),
+                         "how": "full-count steps only (every vertex of the group counted), serialised "
+                                "per-tier CUDA events of %d untimed runs" % PROFILE_RUNS,
+                         "groups": roof.get("groups")},
             "whole_step_roofline": {"bytes_per_iter": int(total_bytes_iter), "iter_ms": round(iter_ms, 4),
                                     "achieved_gbs": round(total_bytes_iter / (iter_ms / 1e3) / 1e9, 1),
                                     "frac": round(total_bytes_iter / (iter_ms / 1e3) / 1e9 / peak, 4)},
@@ -421,6 +493,7 @@ def run_glp(args, ws, rank, local):
             "plan": plan,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "parity": parity,
         }
     handle.close()
     del handle, labels_dev, g
@@ -708,8 +781,8 @@ def run_batched(args, ws, rank, local, embed=False):
                 for g in gs[:k]:
                     path = os.path.join(d, "g.csr")
                     write_csr(path, g.offsets.cpu().numpy(), g.cols.cpu().numpy())
-                    times.append(sum(ref_cpulp_run(path, args.iters)))
-            cpu = {"value": round(k / sum(times), 3), "unit": "graphs/s", "cores": cpu_threads_used(),
+                    times.append(sum(ref_cpulp_run(path, args.iters, cpu_threads())[0]))
+            cpu = {"value": round(k / sum(times), 3), "unit": "graphs/s", "cores": cpu_threads(),
                    "kind": "reference",
                    "sample": f"reference CPUlp::sync_run_1 (tutorial/CPUlp.cuh, built from source), first {k} graphs "
                              f"of the batch x {args.iters} iterations, {sum(times):.2f} s"}

@@ -59,7 +59,8 @@ class Params(C.Structure):
         ("hub_chunk", C.c_int32),
         ("use_graph", C.c_int32),
         ("async_", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("reserved", C.c_int32 * 7),
+        ("serial_step", C.c_int32),
     ]
 
 

@@ -594,7 +594,7 @@ struct glp_batch {
   unsigned int* d_bar = nullptr;
   uint32_t* d_err = nullptr;
   cudaStream_t stream = nullptr;
-  int nsm = 148;
+  int nsm = 1;  // the device's SM count, queried when the batch is created
   glp::Config cfg;
   bool tuned = false;
   // captured launch

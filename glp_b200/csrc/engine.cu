@@ -43,6 +43,23 @@ int cuda_fail(cudaError_t e, const char* what) {
   return e == cudaErrorMemoryAllocation ? GLP_ENOMEM : GLP_ECUDA;
 }
 
+// Streaming multiprocessors of the current device, queried once per device.
+// Grid sizes are multiples of it (a failed query gives 1: the launch that
+// follows reports the device error itself).
+int device_sms() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  if (dev >= 0 && dev < 64) {
+    const int c = cache[dev].load(std::memory_order_relaxed);
+    if (c > 0) return c;
+  }
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) return 1;
+  if (dev >= 0 && dev < 64) cache[dev].store(sms, std::memory_order_relaxed);
+  return sms;
+}
+
 // Device memory of graph handles comes from the device's stream-ordered pool,
 // set once per device to keep freed memory in this process (release
 // threshold at its maximum): handles created and destroyed in a loop reuse
@@ -381,13 +398,6 @@ static int allow_smem(K kernel, size_t bytes) {
 
 static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// GLP_SERIAL_STEP=1 (read at every step) keeps every kernel of a step on one
-// stream, so that per-tier CUDA-event times are the kernels' own durations
-// instead of spans that overlap other tiers (profiling).
-static bool serial_step() {
-  const char* e = std::getenv("GLP_SERIAL_STEP");
-  return e && e[0] == '1';
-}
 
 // One launch over a device-built list of big-tier vertices (majority
 // failures, frontier members, screen fallbacks): 512-thread blocks with a
@@ -397,7 +407,7 @@ static bool serial_step() {
 template <bool W, class S>
 static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWork& tw, const S& score,
                            cudaStream_t s, int64_t* launches) {
-  const unsigned grid = (unsigned)std::min<int64_t>(p.big.n, 148 * 4);
+  const unsigned grid = (unsigned)std::min<int64_t>(p.big.n, device_sms() * 4);
   ++*launches;
   if constexpr (!W) {
     const bool top = p.big_part[kBigParts - 1].n > 0;
@@ -417,7 +427,7 @@ static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWor
 template <bool W, class S>
 int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_t* launches) {
   StepLaunch L = Lin;
-  if (serial_step()) L.aux[0] = L.aux[1] = L.stream;
+  if (L.serial) L.aux[0] = L.aux[1] = L.stream;
   const DevicePlan& p = *L.plan;
   cudaStream_t s = L.stream;
   auto mark_on = [&](cudaStream_t st, int i, int which) -> int {
@@ -425,7 +435,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     return GLP_OK;
   };
   int rc;
-  const unsigned kMaxGrid = 148 * 32;
+  const unsigned kMaxGrid = device_sms() * 32;
   if ((rc = mark_on(s, 8, 0))) return rc;  // whole-step start
   const bool modal = a.mode != nullptr;
   if (modal) {
@@ -434,7 +444,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
                                 L.allow_frontier, p.d_mode);
     ++*launches;
     if (L.allow_frontier && L.front.chg_in) {
-      const unsigned fgrid = 148 * 16;
+      const unsigned fgrid = device_sms() * 16;
       k_frontier_push<<<fgrid, 256, 0, s>>>(a, L.front);
       k_frontier_copy<<<fgrid, 256, 0, s>>>(a, L.front);
       *launches += 2;
@@ -471,7 +481,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     k_hub_gather<kHubNT, W><<<grid, kHubNT, sm_hist, L.aux[0]>>>(a, p.hub, p.n_chunks);
     k_hub_offsets<<<hgrid, 256, 0, L.aux[0]>>>(p.hub);
     k_hub_scatter<kHubNT, W><<<grid, kHubNT, 2 * sm_hist, L.aux[0]>>>(a, p.hub, p.n_chunks);
-    k_hub_bucket<kBucketNT, W, S><<<(unsigned)std::min<int64_t>(p.hub.nitems, 148 * 8), kBucketNT, sm, L.aux[0]>>>(
+    k_hub_bucket<kBucketNT, W, S><<<(unsigned)std::min<int64_t>(p.hub.nitems, device_sms() * 8), kBucketNT, sm, L.aux[0]>>>(
         a, p.hub, score);
     k_hub_finalize<<<hgrid, 256, 0, L.aux[0]>>>(a, p.hub);
     *launches += 6;
@@ -620,6 +630,7 @@ struct RunCtx {
   int64_t launches = 0;
   int iter_base = 0;
   int32_t backend = GLP_BACKEND_EXACT;  // counting back-end of the big tier
+  bool serial = false;                  // glp_params.serial_step: one stream per step
 
   ~RunCtx() {
     for (auto& v : evs)
@@ -657,6 +668,7 @@ struct RunCtx {
     }
     StepLaunch L{&g->plan, s, ev, {g->aux[0], g->aux[1]}, g->fork, {g->join[0], g->join[1]}};
     L.backend = backend;
+    L.serial = serial;
     return L;
   }
   cudaEvent_t* current() { return timing && used ? evs[used - 1].data() : nullptr; }
@@ -767,7 +779,7 @@ static int ensure_sorted(glp_graph* g) {
   uint32_t* d_bad = nullptr;
   GLP_CUDA(dev_alloc(&d_bad, sizeof(uint32_t)));
   GLP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), g->stream));
-  k_check_sorted<<<148 * 32, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, d_bad);
+  k_check_sorted<<<device_sms() * 32, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, d_bad);
   uint32_t bad = 1;
   GLP_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, g->stream));
   GLP_CUDA(cudaStreamSynchronize(g->stream));
@@ -782,7 +794,7 @@ static int ensure_sorted(glp_graph* g) {
 // 32, a warp per mid vertex, a block per big vertex and hub.
 template <bool W>
 static int launch_first_step(const DevicePlan& p, const StepArgs& a, cudaStream_t s, int64_t* launches) {
-  const unsigned kMaxGrid = 148 * 32;
+  const unsigned kMaxGrid = device_sms() * 32;
   if constexpr (!W) {
     k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), kMaxGrid), 256, 0, s>>>(a);
     ++*launches;
@@ -832,7 +844,7 @@ static int ensure_symmetric(glp_graph* g) {
   uint32_t* d_bad = nullptr;
   GLP_CUDA(dev_alloc(&d_bad, sizeof(uint32_t)));
   GLP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), g->stream));
-  k_check_symmetric<<<148 * 16, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, g->m, d_bad);
+  k_check_symmetric<<<device_sms() * 16, 256, 0, g->stream>>>(g->d_off, g->d_cols, g->n, g->m, d_bad);
   uint32_t bad = 1;
   GLP_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, g->stream));
   GLP_CUDA(cudaStreamSynchronize(g->stream));
@@ -1132,7 +1144,7 @@ static int hooks_iterations(RunCtx& c, H h, int32_t niter, int32_t step0, bool l
       h.st.vol_w = *vol_w;
     }
     k_hooks_pick<H><<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(h, g->n);
-    k_hooks_prop<H><<<(unsigned)std::min<int64_t>(cdiv(g->n, 4), 148 * 64), 128, 0, c.s>>>(
+    k_hooks_prop<H><<<(unsigned)std::min<int64_t>(cdiv(g->n, 4), (int64_t)device_sms() * 64), 128, 0, c.s>>>(
         h, g->n, g->d_hook_keys, g->d_hook_vals, g->d_changed + step, g->d_err);
     c.launches += 2;
     GLP_CUDA(cudaGetLastError());
@@ -1195,7 +1207,7 @@ struct NoAllocScratch {
 };
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
-static std::atomic<void*> g_noalloc_ptr[kNoAllocMaxDevices];
+static std::atomic<int> g_noalloc_attr[kNoAllocMaxDevices];  // 1: shared-memory limit raised
 
 static inline size_t pow2_host(int32_t x) {
   size_t p = 1;
@@ -1484,7 +1496,7 @@ int glp_graph_cm_sketch(glp_graph* g, const int32_t* labels, int32_t labels_on_d
   const size_t cells = 3ull * (size_t)width * (size_t)nv;
   int rc = inspect_inputs(g, labels, labels_on_device, vertices, nv, bufs, &d_lab, &d_verts);
   if (rc || (rc = bufs.alloc((void**)&d_rows, sizeof(uint32_t) * cells))) return rc;
-  k_cm_sketch<<<(unsigned)std::min<int32_t>(nv, 148 * 8), 256, 3u * (unsigned)width * sizeof(uint32_t), g->stream>>>(
+  k_cm_sketch<<<(unsigned)std::min<int32_t>(nv, device_sms() * 8), 256, 3u * (unsigned)width * sizeof(uint32_t), g->stream>>>(
       g->d_off, g->d_cols, g->d_w, d_lab, d_verts, nv, width, ref_compat ? 1 : 0, d_rows);
   GLP_CUDA(cudaGetLastError());
   GLP_CUDA(cudaMemcpyAsync(rows, d_rows, sizeof(uint32_t) * cells, cudaMemcpyDeviceToHost, g->stream));
@@ -1610,6 +1622,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.cb = cb;
   c.user = cb_user;
   c.backend = p.backend;
+  c.serial = p.serial_step != 0;
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;
@@ -1688,14 +1701,18 @@ int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int
     set_error("device %d beyond the %d devices the allocation-free path tracks", dev, kNoAllocMaxDevices);
     return GLP_ENOTSUP;
   }
-  // set-up, once per device, with that device current
-  void* sp = g_noalloc_ptr[dev].load(std::memory_order_acquire);
-  if (!sp) {
+  // The scratch's device address, looked up on every call with the device
+  // current (the lookup allocates nothing): a cached address would go stale
+  // if the context were reset and the module loaded again elsewhere.
+  void* sp = nullptr;
+  {
     const cudaError_t e = cudaGetSymbolAddress(&sp, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(allocation-free scratch)");
+  }
+  if (!g_noalloc_attr[dev].load(std::memory_order_acquire)) {
     GLP_CUDA(cudaFuncSetAttribute(k_noalloc_step<kNoAllocNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(2 * pow2_host(2 * kNoAllocMaxDegree) * sizeof(uint32_t))));
-    g_noalloc_ptr[dev].store(sp, std::memory_order_release);
+    g_noalloc_attr[dev].store(1, std::memory_order_release);
   }
   NoAllocScratch* sc = static_cast<NoAllocScratch*>(sp);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1736,7 +1753,7 @@ int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int
   int32_t* buf[2] = {d_labels, sc->labels};
   k_iota<<<(unsigned)cdiv(n, 256), 256, 0, st>>>(buf[0], buf[1], n);
   const size_t smem = 2 * pow2_host(2 * std::max(maxdeg, 1)) * sizeof(uint32_t);
-  const unsigned grid = (unsigned)std::min<int64_t>(n, 148 * 16);
+  const unsigned grid = (unsigned)std::min<int64_t>(n, device_sms() * 16);
   for (int32_t it = 0; it < niter; ++it)
     k_noalloc_step<kNoAllocNT><<<grid, kNoAllocNT, smem, st>>>(d_offsets, d_cols, buf[it & 1], buf[(it + 1) & 1], n,
                                                                sc->changed + it, &sc->err);

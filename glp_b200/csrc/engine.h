@@ -14,6 +14,8 @@ namespace glp {
 
 void set_error(const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
+// Streaming multiprocessors of the current device (queried once per device).
+int device_sms();
 #define GLP_CUDA(call)                                   \
   do {                                                   \
     cudaError_t e_ = (call);                             \
@@ -102,6 +104,7 @@ struct StepLaunch {
   int allow_majority = 0, allow_frontier = 0;
   Frontier front{};  // this step's frontier inputs (front.chg_in set from the second step)
   int32_t backend = GLP_BACKEND_EXACT;  // GLP_BACKEND_CM / _FA: summary screen on the big tier
+  bool serial = false;  // every kernel on `stream` (per-tier timing without overlap)
 };
 
 template <bool W, class S>

@@ -24,6 +24,7 @@
 namespace glp {
 void set_error(const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
+int device_sms();
 }  // namespace glp
 
 namespace {
@@ -143,7 +144,7 @@ int run_sampler(const P& p, int64_t first, int64_t count, int32_t* src, int32_t*
   }
   if (on_device) {
     if (count == 0) return GLP_OK;
-    k_sample<P, F><<<148 * 16, 256>>>(p, first, count, src, dst);
+    k_sample<P, F><<<glp::device_sms() * 16, 256>>>(p, first, count, src, dst);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return glp::cuda_fail(e, "sampler kernel");
@@ -259,7 +260,7 @@ int glp_edge_weights(const int32_t* off, const int32_t* cols, int32_t n, int64_t
   const uint64_t key = mix64(seed ^ 0x27d4eb2full);
   if (on_device) {
     if (n == 0) return GLP_OK;
-    k_weights<<<148 * 8, 256>>>(off, cols, n, wmax, key, w);
+    k_weights<<<glp::device_sms() * 8, 256>>>(off, cols, n, wmax, key, w);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return glp::cuda_fail(e, "weights kernel");

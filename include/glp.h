@@ -96,7 +96,11 @@ typedef struct glp_params {
                                      reported by glp_graph_check(); the
                                      stream must stay valid until the next
                                      call on the handle */
-  int32_t reserved[8];
+  int32_t reserved[7];            /* glp_batch_run reads reserved[0] (threads per block) */
+  int32_t serial_step;            /* 1: every kernel of a step runs on the run's own
+                                     stream instead of three forked streams, so that
+                                     the per-tier event times of glp_outputs are each
+                                     tier's own duration (profiling; slower) */
 } glp_params;
 
 /* Per-iteration observer (parity checks).  labels is a HOST copy of the
@@ -340,11 +344,12 @@ int glp_server_stop(glp_server* s);
  * vertices, niter <= 4096, every degree <= 4096; larger inputs, like a
  * malformed CSR, return GLP_EINVAL with the limit in glp_last_error().
  * `changed` (host, nullable) receives niter change counts.  Work runs on
- * `stream` (NULL: the legacy default stream) and the call returns after it
- * has finished.  The first call on each device looks up that device's scratch
- * (cudaGetSymbolAddress); make it before any stream capture.  The scratch is
- * shared: calls on one device that overlap (from several host threads) race
- * and must be serialised by the caller. */
+ * `stream` (NULL: the legacy default stream) and the call is synchronous: it
+ * returns after that work has finished.  Every call looks up the current
+ * device's copy of the scratch (cudaGetSymbolAddress, which allocates
+ * nothing), so the address stays right after a context reset.  The scratch
+ * is shared: calls on one device that overlap (from several host threads)
+ * race and must be serialised by the caller. */
 int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int32_t n, int64_t m, int32_t niter,
                             int32_t* d_labels, int64_t* changed, void* stream);
 

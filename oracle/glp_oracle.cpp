@@ -33,8 +33,11 @@
 // oracle shares no mechanism with the CUDA kernels it checks.
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
+#include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <utility>
@@ -121,12 +124,42 @@ int orc_classic_step(int32_t n, const int32_t* off, const int32_t* cols, const i
 
 // niter synchronous classic steps from init (NULL: label = vertex id).
 // trace (nullable) receives the labels after every step, [niter][n].
+// From the second step on, a vertex none of whose neighbours changed label
+// in the previous step keeps its label without recounting: its new label is
+// a function of its neighbours' labels only (an isolated vertex keeps its
+// own), and those equal the ones its current label was computed from.  This
+// is exact, needs no symmetry, and makes converged steps cheap.
 int orc_classic_run(int32_t n, const int32_t* off, const int32_t* cols, const int32_t* w, int32_t niter,
                     const int32_t* init, int32_t* lout, int32_t* trace, int nthreads) {
   std::vector<int32_t> a(n), b(n);
+  std::vector<uint8_t> chg(n, 1);
   for (int32_t v = 0; v < n; ++v) a[v] = init ? init[v] : v;
+  const int nt = threads_or_default(nthreads);
   for (int32_t it = 0; it < niter; ++it) {
-    orc_classic_step(n, off, cols, w, a.data(), b.data(), nthreads);
+    if (it == 0) {
+      orc_classic_step(n, off, cols, w, a.data(), b.data(), nthreads);
+    } else {
+#pragma omp parallel num_threads(nt)
+      {
+        std::vector<LW> buf;
+#pragma omp for schedule(dynamic, 1024)
+        for (int32_t v = 0; v < n; ++v) {
+          bool dirty = false;
+          for (int32_t j = off[v]; j < off[v + 1] && !dirty; ++j) dirty = chg[cols[j]] != 0;
+          if (!dirty) {
+            b[v] = a[v];
+            continue;
+          }
+          buf.clear();
+          for (int32_t j = off[v]; j < off[v + 1]; ++j) buf.push_back({a[cols[j]], w ? (int64_t)w[j] : 1});
+          int32_t bl;
+          int64_t bc;
+          b[v] = mode_of(buf, &bl, &bc) ? bl : a[v];
+        }
+      }
+    }
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int32_t v = 0; v < n; ++v) chg[v] = a[v] != b[v];
     std::swap(a, b);
     if (trace) std::memcpy(trace + (size_t)it * n, a.data(), sizeof(int32_t) * n);
   }
@@ -420,6 +453,132 @@ int orc_fa_summary(int32_t v, const int32_t* off, const int32_t* cols, const int
   }
   return rounds;
 }
+
+// ---------------------------------------------------------------- graphs
+// The seeded R-MAT workload built on the host, for the CPU legs of the
+// benchmark (which must not load the engine library) and to check the
+// engine's own sampler + CSR construction: samples as glp_sample_rmat
+// (a counter-based SplitMix64 stream, sample i depends on (seed, i) only;
+// Chakrabarti, Zhan, Faloutsos, "R-MAT", SDM 2004, quadrant probabilities
+// a, b, c, d = 1-a-b-c), then
+//   1. symmetrise (u,v) -> (u,v),(v,u) and drop self loops,
+//   2. sort every row and drop duplicate entries,
+//   3. relabel by degree descending, ties by the smaller original id (the
+//      degree-sorted order tools/normalize.cpp:262-348 produces, made
+//      deterministic),
+//   4. emit int32 offsets[n+1] and int32 columns[m], rows ascending.
+// *off and *cols are malloc'd (free with orc_free).  Returns 0, or -1 on
+// bad parameters / -2 when the graph exceeds an int32 CSR.
+static uint64_t rmat_thresh32(double x) {
+  if (x <= 0) return 0;
+  if (x >= 1) return 1ull << 32;
+  return (uint64_t)std::floor(x * 4294967296.0);
+}
+
+int orc_rmat_csr(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed, int32_t** off_out,
+                 int32_t** cols_out, int64_t* m_out, int nthreads) {
+  if (scale < 1 || scale > 30 || edge_factor < 1 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0) return -1;
+  const int nt = threads_or_default(nthreads);
+  const int64_t n = 1ll << scale;
+  const int64_t count = (int64_t)edge_factor << scale;
+  const uint64_t ta = rmat_thresh32(a), tab = rmat_thresh32(a + b), tabc = rmat_thresh32(a + b + c);
+  const uint64_t key = mix64(seed);
+  std::vector<int32_t> su((size_t)count), sv((size_t)count);
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int64_t i = 0; i < count; ++i) {
+    const uint64_t k = mix64(key ^ (uint64_t)i);
+    uint32_t u = 0, v = 0;
+    uint64_t word = 0;
+    for (int32_t lvl = 0; lvl < scale; ++lvl) {
+      if ((lvl & 1) == 0) word = mix64(k + (uint64_t)(lvl >> 1));
+      const uint64_t r = (lvl & 1) ? (word >> 32) : (word & 0xffffffffull);
+      const uint32_t bu = r < tab ? 0u : 1u;
+      const uint32_t bv = r < ta ? 0u : (r < tab ? 1u : (r < tabc ? 0u : 1u));
+      u = (u << 1) | bu;
+      v = (v << 1) | bv;
+    }
+    su[(size_t)i] = (int32_t)u;
+    sv[(size_t)i] = (int32_t)v;
+  }
+  // 1. symmetrised rows (with duplicates) by counting and scattering
+  std::vector<int64_t> start((size_t)n + 1, 0);
+  {
+    std::vector<std::atomic<int64_t>> deg((size_t)n);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int64_t v = 0; v < n; ++v) deg[(size_t)v].store(0, std::memory_order_relaxed);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int64_t i = 0; i < count; ++i) {
+      if (su[(size_t)i] == sv[(size_t)i]) continue;
+      deg[(size_t)su[(size_t)i]].fetch_add(1, std::memory_order_relaxed);
+      deg[(size_t)sv[(size_t)i]].fetch_add(1, std::memory_order_relaxed);
+    }
+    for (int64_t v = 0; v < n; ++v) start[(size_t)v + 1] = start[(size_t)v] + deg[(size_t)v].load();
+  }
+  std::vector<int32_t> adj((size_t)start[(size_t)n]);
+  {
+    std::vector<std::atomic<int64_t>> cur((size_t)n);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int64_t v = 0; v < n; ++v) cur[(size_t)v].store(start[(size_t)v], std::memory_order_relaxed);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int64_t i = 0; i < count; ++i) {
+      const int32_t u = su[(size_t)i], v = sv[(size_t)i];
+      if (u == v) continue;
+      adj[(size_t)cur[(size_t)u].fetch_add(1, std::memory_order_relaxed)] = v;
+      adj[(size_t)cur[(size_t)v].fetch_add(1, std::memory_order_relaxed)] = u;
+    }
+  }
+  std::vector<int32_t>().swap(su);
+  std::vector<int32_t>().swap(sv);
+  // 2. sort + dedupe every row in place; ddeg = deduplicated degree
+  std::vector<int64_t> ddeg((size_t)n);
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(nt)
+  for (int64_t v = 0; v < n; ++v) {
+    int32_t* b0 = adj.data() + start[(size_t)v];
+    int32_t* e0 = adj.data() + start[(size_t)v + 1];
+    std::sort(b0, e0);
+    ddeg[(size_t)v] = std::unique(b0, e0) - b0;
+  }
+  // 3. degree-descending order, stable in the original id (counting sort)
+  int64_t maxd = 0;
+  for (int64_t v = 0; v < n; ++v) maxd = std::max(maxd, ddeg[(size_t)v]);
+  std::vector<int64_t> bucket((size_t)maxd + 2, 0);
+  for (int64_t v = 0; v < n; ++v) ++bucket[(size_t)(maxd - ddeg[(size_t)v]) + 1];
+  for (int64_t d = 0; d <= maxd; ++d) bucket[(size_t)d + 1] += bucket[(size_t)d];
+  std::vector<int32_t> perm((size_t)n), newid((size_t)n);
+  for (int64_t v = 0; v < n; ++v) {
+    const int64_t pos = bucket[(size_t)(maxd - ddeg[(size_t)v])]++;
+    perm[(size_t)pos] = (int32_t)v;
+    newid[(size_t)v] = (int32_t)pos;
+  }
+  // 4. the relabelled CSR, rows ascending
+  int64_t m = 0;
+  for (int64_t v = 0; v < n; ++v) m += ddeg[(size_t)v];
+  if (m > INT32_MAX) return -2;
+  int32_t* off = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t)(n + 1)));
+  int32_t* cols = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1)));
+  if (!off || !cols) {
+    std::free(off);
+    std::free(cols);
+    return -3;
+  }
+  off[0] = 0;
+  for (int64_t r = 0; r < n; ++r) off[r + 1] = off[r] + (int32_t)ddeg[(size_t)perm[(size_t)r]];
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(nt)
+  for (int64_t r = 0; r < n; ++r) {
+    const int32_t v = perm[(size_t)r];
+    const int32_t* src = adj.data() + start[(size_t)v];
+    int32_t* dst = cols + off[r];
+    const int64_t d = ddeg[(size_t)v];
+    for (int64_t j = 0; j < d; ++j) dst[j] = newid[(size_t)src[j]];
+    std::sort(dst, dst + d);
+  }
+  *off_out = off;
+  *cols_out = cols;
+  *m_out = m;
+  return 0;
+}
+
+void orc_free(void* p) { std::free(p); }
 
 // Number of vertices whose label differs between two arrays.
 int64_t orc_count_diff(int32_t n, const int32_t* a, const int32_t* b) {

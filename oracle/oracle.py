@@ -50,6 +50,9 @@ def load():
     lib.orc_cm_estimate.restype = C.c_uint32
     lib.orc_cm_estimate.argtypes = [vp, C.c_int32, C.c_int, C.c_int32]
     lib.orc_fa_summary.argtypes = [C.c_int32, vp, vp, vp, C.c_int32, C.c_int, vp, vp]
+    lib.orc_rmat_csr.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                 C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.c_int]
+    lib.orc_free.argtypes = [vp]
     lib.orc_count_diff.restype = C.c_int64
     lib.orc_count_diff.argtypes = [C.c_int32, vp, vp]
     _lib = lib
@@ -166,3 +169,24 @@ def fa_summary(v: int, off, cols, labels, C_: int, ref_compat: bool = False):
     vals = np.empty(C_, dtype=np.uint32)
     rounds = load().orc_fa_summary(v, _p(off), _p(cols), _p(lab), C_, int(ref_compat), _p(keys), _p(vals))
     return keys, vals, rounds
+
+
+def rmat_csr(scale: int, edge_factor: int = 16, seed: int = 1, abc=(0.57, 0.19, 0.19), threads: int = 0):
+    """The seeded R-MAT workload as an int32 CSR built on the host (the
+    engine's sampler restated; symmetrised, self loops and duplicates dropped,
+    degree-descending relabel, rows ascending): (offsets, cols)."""
+    lib = load()
+    po, pc, m = C.c_void_p(), C.c_void_p(), C.c_int64()
+    a, b, c = abc
+    rc = lib.orc_rmat_csr(scale, edge_factor, a, b, c, seed, C.byref(po), C.byref(pc), C.byref(m), threads)
+    if rc != 0:
+        raise ValueError(f"orc_rmat_csr failed ({rc})")
+    n = 1 << scale
+    try:
+        off = np.ctypeslib.as_array(C.cast(po, C.POINTER(C.c_int32)), (n + 1,)).copy()
+        cols = (np.ctypeslib.as_array(C.cast(pc, C.POINTER(C.c_int32)), (m.value,)).copy()
+                if m.value else np.zeros(0, np.int32))
+    finally:
+        lib.orc_free(po)
+        lib.orc_free(pc)
+    return off, cols

@@ -10,9 +10,20 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+# Runs the reference arm in this process and then lists the shared objects the
+# process mapped: the reference arm must not load the engine library.
+_ARM = """
+import json, sys
+sys.argv = ["bench.py", "--impl", "reference", "--scale", "10", "--steps", "2", "--warmup", "1"]
+import bench
+bench.main()
+maps = open("/proc/self/maps").read()
+print("ENGINE_LOADED" if "libglp_b200" in maps else "ENGINE_NOT_LOADED")
+"""
+
+
 def test_reference_arm_prints_one_contract_line():
-    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--scale", "10", "--steps", "2",
-                        "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    r = subprocess.run([sys.executable, "-c", _ARM], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
@@ -25,8 +36,24 @@ def test_reference_arm_prints_one_contract_line():
                 "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert key in line, key
     assert line["value"] > 0 and line["unit"] == "GTEPS" and line["higher_is_better"] is True
-    assert line["steps"] == 2 and line["warmup"] == 1
+    assert "ENGINE_NOT_LOADED" in r.stdout  # the graph is built by the oracle, not by libglp_b200.so
+    assert line["steps"] == 2 and line["warmup"] == 0
     assert line["config"]["n"] == 1024 and line["config"]["workload"] == "rmat10-ef16-seed2-classic-20it"
     assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"] == {"value": line["value"], "unit": "GTEPS", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_host_rmat_csr_equals_engine_sampler_csr():
+    """The oracle's host R-MAT build (used by the CPU legs of the benchmark) is
+    byte-identical to the engine's sampler + CSR construction."""
+    import numpy as np
+
+    from glp_b200 import graphs
+    from oracle import oracle as O
+
+    for scale, seed in ((9, 1), (12, 2)):
+        off, cols = O.rmat_csr(scale, 16, seed=seed)
+        o2, c2, _ = graphs.rmat(scale, 16, seed=seed, device="cpu").numpy()
+        np.testing.assert_array_equal(off, o2)
+        np.testing.assert_array_equal(cols, c2)
