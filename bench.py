@@ -798,7 +798,7 @@ def run_batched(args, ws, rank, local, embed=False):
                    "graphs": args.graphs, "n": n, "m": m, "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (CSR %.1f GB); no flush" % (4 * (n + 1 + m) / 1e9),
                    "launch": "one persistent cooperative launch per step, CUDA-graph replay",
-                   "tuned": {"threads": best.reserved[0], "thread_tier_max": best.tiny_max,
+                   "tuned": {"threads": best.batch_threads, "thread_tier_max": best.tiny_max,
                              "warp_tier_max": best.mid_max},
                    "tune_s": round(tune_s, 2), "graph_gen_s": round(gen_s, 2)},
         "plain": {"value": round(plain_value, 1), "unit": "graphs/s", "sample_graphs": len(idx),

@@ -59,7 +59,10 @@ class Params(C.Structure):
         ("hub_chunk", C.c_int32),
         ("use_graph", C.c_int32),
         ("async_", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("batch_threads", C.c_int32),
+        ("barrier_limit_us", C.c_int32),
+        ("fault_skip_cta", C.c_int32),
+        ("reserved", C.c_int32 * 4),
         ("serial_step", C.c_int32),
     ]
 
@@ -95,6 +98,8 @@ SIGNATURES = {
     "glp_graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "glp_graph_plan": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(C.c_int64)]),
     "glp_graph_check": (C.c_int, [C.c_void_p]),
+    "glp_graph_device_view": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "glp_graph_set_cancel_flag": (C.c_int, [C.c_void_p, C.c_void_p]),
     "glp_graph_cm_sketch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                                       C.c_void_p]),
     "glp_graph_fa_summary": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,
@@ -136,6 +141,7 @@ SIGNATURES = {
     "glp_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p]),
     "glp_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
     "glp_server_release": (C.c_int, [C.c_void_p, C.c_int64]),
+    "glp_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
     "glp_server_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                   C.POINTER(C.c_int64)]),
     "glp_server_stop": (C.c_int, [C.c_void_p]),

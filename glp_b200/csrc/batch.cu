@@ -59,7 +59,7 @@ namespace {
 constexpr int32_t kBatchMaxDegree = 4096;
 constexpr uint32_t kErrBarrier = 8u;   // a grid barrier ran out of time
 constexpr uint32_t kBadOffsets = 1u, kBadCols = 2u, kBadDegree = 4u, kUnsortedRow = 8u;
-constexpr unsigned long long kBarrierLimitNs = 5000000000ull;  // 5 s
+constexpr unsigned long long kBarrierLimitNs = 5000000000ull;  // default wait limit: 5 s
 
 struct BatchArgs {
   const int64_t* off;      // [N+1] global row offsets
@@ -82,6 +82,8 @@ struct BatchArgs {
   uint32_t* err;
   int32_t niter;
   int32_t first_step;      // rows strictly ascending
+  unsigned long long barrier_ns;  // how long a grid barrier waits before giving up
+  int32_t skip_cta;        // failure tests: 1 + a CTA that never arrives at the first barrier (0: none)
 };
 
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -98,13 +100,16 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
 
 // Grid barrier of a cooperative launch: CTA leaders add to a counter that
 // never resets (phase p waits for (p+1)*gridDim.x arrivals).  A leader gives
-// up after kBarrierLimitNs, or as soon as another CTA has given up.
-__device__ bool grid_barrier(unsigned int* bar, unsigned int target, uint32_t* err) {
+// up after limit_ns of %globaltimer, or as soon as another CTA has given up;
+// either way the kernel then returns with kErrBarrier set.  `arrive` = false
+// withholds this CTA's arrival (failure tests: nobody's wait can be met).
+__device__ bool grid_barrier(unsigned int* bar, unsigned int target, uint32_t* err,
+                             unsigned long long limit_ns = kBarrierLimitNs, bool arrive = true) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    atomicAdd(bar, 1u);
+    if (arrive) atomicAdd(bar, 1u);
     const uint64_t t0 = globaltimer();
     int ok = 1;
     while (ld_acquire(bar) < target) {
@@ -112,7 +117,7 @@ __device__ bool grid_barrier(unsigned int* bar, unsigned int target, uint32_t* e
         ok = 0;
         break;
       }
-      if (globaltimer() - t0 > kBarrierLimitNs) {
+      if (globaltimer() - t0 > limit_ns) {
         atomicOr(err, kErrBarrier);
         ok = 0;
         break;
@@ -389,7 +394,8 @@ __global__ void __launch_bounds__(NT) k_batch(BatchArgs a) {
     }
     if (a.first_step && a.niter > 0) block_count_add<NT>(a.changed, chg, red_u);
   }
-  if (!grid_barrier(a.bar, ++phase * gridDim.x, a.err)) return;
+  if (!grid_barrier(a.bar, ++phase * gridDim.x, a.err, a.barrier_ns, (int32_t)blockIdx.x + 1 != a.skip_cta))
+    return;
 
   uint32_t* smem_warp = smem + (size_t)warp * a.warp_words;
   for (int32_t it = a.first_step ? 1 : 0; it < a.niter; ++it) {
@@ -416,7 +422,7 @@ __global__ void __launch_bounds__(NT) k_batch(BatchArgs a) {
       chg += sweep_threads<NT, 8>(a, B[6], B[7], lin, lout);
     }
     block_count_add<NT>(a.changed + it, chg, red_u);
-    if (it + 1 < a.niter && !grid_barrier(a.bar, ++phase * gridDim.x, a.err)) return;
+    if (it + 1 < a.niter && !grid_barrier(a.bar, ++phase * gridDim.x, a.err, a.barrier_ns)) return;
   }
 }
 
@@ -555,7 +561,11 @@ struct Config {
   int nt = 1024;   // threads per CTA
   int tt = 32;     // degrees <= tt: a thread per vertex (8, 16 or 32)
   int half = 1;    // degrees 33..64: 16-lane groups (else whole warps)
-  bool operator==(const Config& o) const { return nt == o.nt && tt == o.tt && half == o.half; }
+  unsigned long long barrier_ns = kBarrierLimitNs;  // grid-barrier wait limit
+  int skip_cta = 0;  // failure tests: 1 + a CTA withholding its first arrival
+  bool operator==(const Config& o) const {
+    return nt == o.nt && tt == o.tt && half == o.half && barrier_ns == o.barrier_ns && skip_cta == o.skip_cta;
+  }
 };
 
 }  // namespace
@@ -686,6 +696,8 @@ BatchArgs make_args(glp_batch* b, const Config& c, int32_t niter) {
   a.err = b->d_err;
   a.niter = max_niter(b, niter);
   a.first_step = b->first_step;
+  a.barrier_ns = c.barrier_ns;
+  a.skip_cta = c.skip_cta;
   return a;
 }
 
@@ -730,7 +742,9 @@ Config config_from(const glp_batch* b, const glp_params* p) {
     if (p->tiny_max == 8 || p->tiny_max == 16 || p->tiny_max == 32) c.tt = p->tiny_max;
     if (p->mid_max == 32) c.half = 0;
     if (p->mid_max == 64) c.half = 1;
-    if (p->reserved[0] == 512 || p->reserved[0] == 1024) c.nt = p->reserved[0];
+    if (p->batch_threads == 512 || p->batch_threads == 1024) c.nt = p->batch_threads;
+    c.barrier_ns = p->barrier_limit_us > 0 ? 1000ull * (unsigned long long)p->barrier_limit_us : kBarrierLimitNs;
+    c.skip_cta = p->fault_skip_cta > 0 ? p->fault_skip_cta : 0;
   }
   return c;
 }
@@ -1143,7 +1157,7 @@ int glp_batch_tune(glp_batch* b, int32_t probe_iters, glp_params* best, float* t
     glp_params_default(best);
     best->tiny_max = best_c.tt;
     best->mid_max = best_c.half ? 64 : 32;
-    best->reserved[0] = best_c.nt;
+    best->batch_threads = best_c.nt;
   }
   return GLP_OK;
 }

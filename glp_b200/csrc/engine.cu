@@ -721,6 +721,13 @@ static int check_err(glp_graph* g, cudaStream_t s) {
 
 static int after_iter(RunCtx& c, int32_t iter, const int32_t* d_labels) {
   int rc;
+  if (c.g->cancel && *c.g->cancel) {
+    // stop enqueuing; the work already on the stream finishes first, so the
+    // handle has nothing in flight when the call returns
+    GLP_CUDA(cudaStreamSynchronize(c.s));
+    set_error("run cancelled after iteration %d", iter);
+    return GLP_ECANCELED;
+  }
   if (!c.cb) return GLP_OK;
   c.hbuf.resize(c.g->n);
   GLP_CUDA(cudaMemcpyAsync(c.hbuf.data(), d_labels, sizeof(int32_t) * c.g->n, cudaMemcpyDeviceToHost, c.s));
@@ -1143,9 +1150,9 @@ static int hooks_iterations(RunCtx& c, H h, int32_t niter, int32_t step0, bool l
       h.st.vol_r = *vol_r;
       h.st.vol_w = *vol_w;
     }
-    k_hooks_pick<H><<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(h, g->n);
-    k_hooks_prop<H><<<(unsigned)std::min<int64_t>(cdiv(g->n, 4), (int64_t)device_sms() * 64), 128, 0, c.s>>>(
-        h, g->n, g->d_hook_keys, g->d_hook_vals, g->d_changed + step, g->d_err);
+    glp_hooks::k_pick<H><<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(h, g->n);
+    glp_hooks::k_prop<H><<<(unsigned)std::min<int64_t>(cdiv(g->n, 4), (int64_t)device_sms() * 64), 128, 0, c.s>>>(
+        h, h.st, g->d_hook_keys, g->d_hook_vals, g->d_changed + step, g->d_err);
     c.launches += 2;
     GLP_CUDA(cudaGetLastError());
     if ((rc = after_iter(c, step, h.st.Lnext))) return rc;
@@ -1159,7 +1166,7 @@ static int run_hooks(RunCtx& c, const glp_params& p, int32_t niter) {
     GLP_CUDA(dev_alloc(&g->d_hook_keys, sizeof(uint32_t) * 2 * (size_t)g->m));
     GLP_CUDA(dev_alloc(&g->d_hook_vals, sizeof(double) * 2 * (size_t)g->m));
   }
-  HookState st{g->d_off, g->d_cols, g->d_w, g->d_lab[0], g->d_lab[1], nullptr, nullptr, 1.0};
+  HookState st{g->d_off, g->d_cols, g->d_w, g->n, g->d_lab[0], g->d_lab[1], nullptr, nullptr, 1.0, nullptr};
   c.iter_base = 1;  // Lnext holds the final labels
   int rc;
   if (p.hooks == GLP_HOOKS_LAYERED) {
@@ -1437,6 +1444,55 @@ int glp_graph_check(glp_graph* g) {
   }
   if (!g->d_err) return GLP_OK;
   return check_err(g, g->stream);
+}
+
+int glp_graph_set_cancel_flag(glp_graph* g, const volatile int32_t* flag) {
+  if (!g) {
+    set_error("graph is NULL");
+    return GLP_EINVAL;
+  }
+  g->cancel = flag;
+  return GLP_OK;
+}
+
+int glp_graph_device_view(glp_graph* g, int32_t niter, glp_device_view* out) {
+  if (!g || !out || niter < 0) {
+    set_error("graph, output and niter >= 0 are required");
+    return GLP_EINVAL;
+  }
+  GLP_CUDA(cudaSetDevice(g->device));
+  int rc;
+  if ((rc = quiesce(g))) return rc;
+  if ((rc = ensure_work(g, niter))) return rc;
+  if (g->max_degree > kHookSmemCap / 2 && !g->d_hook_keys) {
+    GLP_CUDA(dev_alloc(&g->d_hook_keys, sizeof(uint32_t) * 2 * (size_t)g->m));
+    GLP_CUDA(dev_alloc(&g->d_hook_vals, sizeof(double) * 2 * (size_t)g->m));
+  }
+  if (g->n) {
+    k_iota<<<(unsigned)cdiv(g->n, 256), 256, 0, g->stream>>>(g->d_lab[0], g->d_lab[1], g->n);
+    GLP_CUDA(cudaGetLastError());
+  }
+  GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (niter + 1), g->stream));
+  GLP_CUDA(cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), g->stream));
+  GLP_CUDA(cudaStreamSynchronize(g->stream));
+  glp_device_view v{};
+  v.n = g->n;
+  v.max_degree = g->max_degree;
+  v.m = g->m;
+  v.device = g->device;
+  v.sms = device_sms();
+  v.off = g->d_off;
+  v.cols = g->d_cols;
+  v.w = g->d_w;
+  v.labels[0] = g->d_lab[0];
+  v.labels[1] = g->d_lab[1];
+  v.changed = g->d_changed;
+  v.err = g->d_err;
+  v.hook_keys = g->d_hook_keys;
+  v.hook_vals = g->d_hook_vals;
+  v.stream = g->stream;
+  *out = v;
+  return GLP_OK;
 }
 
 // Device buffers of one summary inspection call, freed on every return path.

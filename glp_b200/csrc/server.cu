@@ -82,6 +82,7 @@ struct Request {
   bool batched = false;
   int64_t bytes = 0;
   double cost_s = 0;  // expected service time, for shortest-job-first
+  volatile int32_t cancel = 0;  // glp_server_cancel: stop (one-graph solve) or discard (batched round)
   // results
   int32_t status = GLP_EAGAIN;
   std::string error;
@@ -154,8 +155,8 @@ void release_graph_locked(glp_server* s, Resident* g) {
   }
 }
 
-void finish(glp_server* s, Request* r, int status, const char* err) {
-  std::lock_guard<std::mutex> lk(s->mu);
+// Caller holds s->mu.
+void finish_locked(glp_server* s, Request* r, int status, const char* err) {
   r->status = status;
   if (err) r->error = err;
   r->stats.done_s = s->now();
@@ -164,6 +165,11 @@ void finish(glp_server* s, Request* r, int status, const char* err) {
   s->in_flight--;
   release_graph_locked(s, r->res);
   r->res = nullptr;
+}
+
+void finish(glp_server* s, Request* r, int status, const char* err) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  finish_locked(s, r, status, err);
 }
 
 // Moves pending requests that fit the budget to their path (FIFO: the head
@@ -252,10 +258,16 @@ void plain_worker(glp_server* s) {
     } else {
       rc = glp_graph_create(r->offsets, r->cols, r->weights, r->n, r->m, 0, &g);
     }
+    if (rc == GLP_OK && r->cancel) {
+      glp::set_error("cancelled before it started");
+      rc = GLP_ECANCELED;
+    }
     if (rc == GLP_OK) {
       glp_outputs out{};
       out.labels = r->labels;
+      glp_graph_set_cancel_flag(g, &r->cancel);
       rc = glp_run(g, r->method, &r->params, r->niter, &out, nullptr, nullptr, nullptr);
+      glp_graph_set_cancel_flag(g, nullptr);
     }
     const std::string err = rc ? glp_last_error() : std::string();
     if (transient) glp_graph_destroy(g);
@@ -348,6 +360,11 @@ void batch_worker(glp_server* s) {
     s->rounds++;
     int64_t base = 0;
     for (Request* r : round) {
+      if (r->cancel) {  // cancelled while its round ran: the result is discarded
+        base += r->n;
+        finish(s, r, GLP_ECANCELED, "cancelled during its batched round");
+        continue;
+      }
       if (rc == GLP_OK && r->n) std::memcpy(r->labels, packed.data() + base, sizeof(int32_t) * (size_t)r->n);
       base += r->n;
       finish(s, r, rc, rc ? err.c_str() : nullptr);
@@ -664,6 +681,45 @@ int glp_server_release(glp_server* s, int64_t id) {
     return GLP_EINVAL;
   }
   s->all.erase(it);
+  return GLP_OK;
+}
+
+int glp_server_cancel(glp_server* s, int64_t id) {
+  if (!s) {
+    set_error("server is NULL");
+    return GLP_EINVAL;
+  }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) {
+      set_error("unknown request %lld", (long long)id);
+      return GLP_EINVAL;
+    }
+    Request* r = it->second.get();
+    if (r->status != GLP_EAGAIN) return GLP_OK;  // already finished: its result stands
+    r->cancel = 1;
+    auto take = [&](std::deque<Request*>& q) {
+      auto f = std::find(q.begin(), q.end(), r);
+      if (f == q.end()) return false;
+      q.erase(f);
+      return true;
+    };
+    if (take(s->pending)) {  // never admitted: it holds no budget
+      r->status = GLP_ECANCELED;
+      r->error = "cancelled before admission";
+      r->stats.done_s = s->now();
+      r->stats.status = GLP_ECANCELED;
+      release_graph_locked(s, r->res);
+      r->res = nullptr;
+    } else if (take(s->batch_q) || take(s->plain_q)) {
+      finish_locked(s, r, GLP_ECANCELED, "cancelled before it started");
+    }
+    // otherwise it is running: its worker sees r->cancel
+    admit_locked(s);
+  }
+  s->cv_done.notify_all();
+  s->cv_work.notify_all();
   return GLP_OK;
 }
 

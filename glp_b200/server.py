@@ -129,10 +129,22 @@ class Server:
         _lib.check(rc)
         return st.as_dict()
 
+    def stats(self, r: Request) -> tuple[int, dict]:
+        """(status, timestamps) of a request, done or not (GLP_EAGAIN while it
+        waits or runs; start_s stays 0 until it starts)."""
+        st = RequestStats()
+        rc = self._lib.glp_server_poll(self._h, r.id, C.byref(st))
+        return rc, st.as_dict()
+
     def wait(self, r: Request, timeout_ms: int = -1) -> dict:
         st = RequestStats()
         _lib.check(self._lib.glp_server_wait(self._h, r.id, timeout_ms, C.byref(st)))
         return st.as_dict()
+
+    def cancel(self, r: Request) -> None:
+        """Cancel a request (glp_server_cancel); wait() then reports GLP_ECANCELED
+        unless it had already finished."""
+        _lib.check(self._lib.glp_server_cancel(self._h, r.id))
 
     def release(self, r: Request) -> None:
         _lib.check(self._lib.glp_server_release(self._h, r.id))

@@ -96,7 +96,13 @@ typedef struct glp_params {
                                      reported by glp_graph_check(); the
                                      stream must stay valid until the next
                                      call on the handle */
-  int32_t reserved[7];            /* glp_batch_run reads reserved[0] (threads per block) */
+  int32_t batch_threads;          /* glp_batch_run: threads per block, 512 or 1024 (0 = tuned / default) */
+  int32_t barrier_limit_us;       /* glp_batch_run: how long a grid barrier of the persistent kernel
+                                     waits before the run gives up with GLP_ETIMEOUT (0 = 5 s) */
+  int32_t fault_skip_cta;         /* glp_batch_run, for tests of the failure path: 1 + the index of a
+                                     block that never arrives at the first grid barrier, so that the
+                                     other blocks' bounded waits run out (0 = off) */
+  int32_t reserved[4];
   int32_t serial_step;            /* 1: every kernel of a step runs on the run's own
                                      stream instead of three forked streams, so that
                                      the per-tier event times of glp_outputs are each
@@ -162,6 +168,34 @@ int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int
 /* Reports (and clears) kernel error flags raised by asynchronous runs. */
 int glp_graph_check(glp_graph* g);
 
+/* Device view of a handle for method-4 hook sets compiled outside the
+ * library (include/glp_hooks.cuh).  Replaces the reference's route for user
+ * hooks -- editing the __device__ stubs of header/kernel.cuh:6071-6085 and
+ * rebuilding (README.md:72-101) -- with a resident graph that user code
+ * reads in place. */
+typedef struct glp_device_view {
+  int32_t n;
+  int32_t max_degree;
+  int64_t m;
+  int32_t device;               /* CUDA device of the handle */
+  int32_t sms;                  /* its streaming multiprocessors */
+  const int32_t* off;           /* [n+1] device CSR offsets */
+  const int32_t* cols;          /* [m] device CSR columns */
+  const int32_t* w;             /* [m] device weights, NULL when unweighted */
+  int32_t* labels[2];           /* [n] each: both set to the vertex ids */
+  unsigned long long* changed;  /* [niter] per-iteration change counters, zeroed */
+  uint32_t* err;                /* one error word, zeroed */
+  uint32_t* hook_keys;          /* [2m] spill table keys for degrees above 256 (else NULL) */
+  double* hook_vals;            /* [2m] spill table values (else NULL) */
+  void* stream;                 /* the handle's stream */
+} glp_device_view;
+/* Prepares the handle's buffers for a run of niter iterations written outside
+ * the library and fills *out: label buffers (set to the vertex ids), niter
+ * change counters and the error word (zeroed), and the spill tables when a
+ * degree exceeds 256.  The pointers stay valid until the next call on the
+ * handle or glp_graph_destroy.  Synchronous. */
+int glp_graph_device_view(glp_graph* g, int32_t niter, glp_device_view* out);
+
 /* ---- counting summaries on the device (parity inspection) --------------
  * The count-min sketch SharedCM<W,3> of method/countmin.cuh:9-262 built over
  * the whole neighbourhood of each listed vertex under `labels` (n entries,
@@ -183,6 +217,13 @@ int glp_graph_cm_sketch(glp_graph* g, const int32_t* labels, int32_t labels_on_d
 int glp_graph_fa_summary(glp_graph* g, const int32_t* labels, int32_t labels_on_device, const int32_t* vertices,
                          int32_t nv, int32_t capacity, int32_t ref_compat, uint32_t* keys, uint32_t* vals,
                          int32_t* rounds);
+
+/* Cancellation of runs on this handle: while flag (host memory, NULL = none)
+ * is non-zero, glp_run stops at the next iteration boundary with
+ * GLP_ECANCELED, after the work it already enqueued has finished (the
+ * handle then has nothing in flight).  Another thread may set the flag at
+ * any time.  No counterpart in the reference (its runs cannot be stopped). */
+int glp_graph_set_cancel_flag(glp_graph* g, const volatile int32_t* flag);
 
 /* Run `method` for niter iterations (layered: nlayers*niter).  Replaces
  * XProp<V,E>::run(niter) of prop/classicLprop.cuh:454-462,
@@ -262,7 +303,7 @@ int glp_batch_info(const glp_batch* b, int64_t* n, int64_t* m, int32_t* max_degr
  * values = the tuned or default choice): tiny_max in {8,16,32} = largest
  * degree counted by one thread per vertex (above it, up to 32, lane groups);
  * mid_max 64 = degrees 33..64 by 16-lane groups, 32 = by whole warps;
- * reserved[0] in {512,1024} = threads per block; use_graph = 1 captures the
+ * batch_threads in {512,1024} = threads per block; use_graph = 1 captures the
  * run (counter resets, the persistent launch, a device-side label copy) in a
  * CUDA graph once and replays it while niter, the configuration, the stream
  * and the device label pointer stay the same.  Synchronous with respect to
@@ -328,6 +369,13 @@ int glp_server_poll(glp_server* s, int64_t id, glp_request_stats* stats);
 int glp_server_wait(glp_server* s, int64_t id, int32_t timeout_ms, glp_request_stats* stats);
 /* Forgets a finished request. */
 int glp_server_release(glp_server* s, int64_t id);
+/* Cancels a request: one still waiting for admission, or admitted and not
+ * started, ends at once with GLP_ECANCELED and gives back its budget; a
+ * one-graph solve in progress stops at its next iteration boundary; a request
+ * already inside a batched round finishes that round and its result is
+ * discarded.  Either way the request then reports GLP_ECANCELED, unless it
+ * had already finished (its result stands).  GLP_EINVAL for an unknown id. */
+int glp_server_cancel(glp_server* s, int64_t id);
 int glp_server_info(glp_server* s, int64_t* pending, int64_t* in_flight, int64_t* used_bytes, int64_t* rounds);
 /* Finishes every submitted request, then stops the threads and frees. */
 int glp_server_stop(glp_server* s);

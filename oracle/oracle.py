@@ -190,3 +190,106 @@ def rmat_csr(scale: int, edge_factor: int = 16, seed: int = 1, abc=(0.57, 0.19, 
         lib.orc_free(po)
         lib.orc_free(pc)
     return off, cols
+
+
+# ---------------------------------------------------------------- reference GPU kernels
+REF_GPU_EXE = os.path.join(HERE, "_ref", "ref_gpu_lp")
+
+
+def _write_csr(path, off, cols):
+    with open(path, "wb") as f:
+        np.array([len(off) - 1, len(cols)], dtype=np.int64).tofile(f)
+        np.ascontiguousarray(off, dtype=np.int32).tofile(f)
+        np.ascontiguousarray(cols, dtype=np.int32).tofile(f)
+
+
+def ref_gpu_classic(off, cols, niter: int, init=None):
+    """The reference's own classic kernels (header/kernel.cuh, driven by
+    oracle/ref_gpu_harness.cu) for niter synchronous steps from `init`
+    (label = id when None): labels after every step, [niter][n].  Needs a
+    GPU and a degree-sorted CSR."""
+    import tempfile
+    off, cols, _ = _csr(off, cols, None)
+    n = len(off) - 1
+    with tempfile.TemporaryDirectory() as d:
+        g, tr, ini = os.path.join(d, "g.csr"), os.path.join(d, "t.bin"), "-"
+        _write_csr(g, off, cols)
+        if init is not None:
+            ini = os.path.join(d, "init.bin")
+            np.ascontiguousarray(init, dtype=np.int32).tofile(ini)
+        subprocess.run([REF_GPU_EXE, "classic", g, str(niter), ini, tr], check=True, capture_output=True, timeout=600)
+        return np.fromfile(tr, dtype=np.int32).reshape(niter, n)
+
+
+def ref_gpu_layered(off, cols, dstar, niter: int):
+    """The reference's own layered kernels (ml_*, header/kernel.cuh) driven
+    by oracle/ref_gpu_harness.cu with the oracle's volume bookkeeping:
+    (labels after every step [len(dstar)*niter][n], volumes after the last)."""
+    import tempfile
+    off, cols, _ = _csr(off, cols, None)
+    n = len(off) - 1
+    with tempfile.TemporaryDirectory() as d:
+        g, tr, vol = os.path.join(d, "g.csr"), os.path.join(d, "t.bin"), os.path.join(d, "v.bin")
+        _write_csr(g, off, cols)
+        subprocess.run([REF_GPU_EXE, "layered", g, str(niter), ",".join(str(int(x)) for x in dstar), tr, vol],
+                       check=True, capture_output=True, timeout=600)
+        return np.fromfile(tr, dtype=np.int32).reshape(len(dstar) * niter, n), np.fromfile(vol, dtype=np.int32)
+
+
+def ref_gpu_tier(degree: int) -> str:
+    """The reference's degree tier of a vertex (prop/classicLprop.cuh:196-227):
+    huge > 640 >= big > 128 >= medium > 32 >= small > 16 >= tiny."""
+    if degree > 640:
+        return "huge"
+    if degree > 128:
+        return "big"
+    if degree > 32:
+        return "medium"
+    if degree > 16:
+        return "small"
+    return "tiny"
+
+
+def ref_medium_choice(keys) -> int:
+    """The label l_medium_update_syn_labelload picks for one vertex of degree
+    33..128 from its neighbours' keys (label + 1) in CSR order
+    (header/kernel.cuh:3156-3218), restated lane by lane: the warp reads 32
+    neighbours per round; in each round the lowest lane holding a key adds
+    the round's occurrences of that key to the key's running total; a lane
+    keeps the (total, key) of an insert only when the total is strictly
+    larger than what it holds (from (0, 0)), so a later key reaching the same
+    total on the same lane is dropped; the warp then takes the largest
+    (total << 32 | key).  Returns the label (key - 1).  Pure Python: for
+    small cases."""
+    keys = [int(k) for k in keys]
+    total = {}
+    best = [(0, 0)] * 32
+    for r in range(0, len(keys), 32):
+        chunk = keys[r:r + 32]
+        for lane, k in enumerate(chunk):
+            if k in chunk[:lane]:
+                continue
+            t = total.get(k, 0) + chunk.count(k)
+            total[k] = t
+            if best[lane][0] < t:
+                best[lane] = (t, k)
+    return max(best)[1] - 1
+
+
+def ref_gpu_slpa(off, cols, T: int, niter: int, seed: int):
+    """SLPA with the reference's own speaker memory (tutorial/Base5prop.cuh:
+    161-208 storelabel/picklabel, rand() replaced by the counter hash H(seed,
+    iteration, v)) and a host listener with the synchronous rule, run by
+    oracle/ref_gpu_harness.cu: (labels after every step [niter][n], memory
+    [T][n] with -1 for an empty slot).  Needs a GPU (the reference's steps
+    copy labels to and from the device)."""
+    import tempfile
+    off, cols, _ = _csr(off, cols, None)
+    n = len(off) - 1
+    with tempfile.TemporaryDirectory() as d:
+        g, tr, mem = os.path.join(d, "g.csr"), os.path.join(d, "t.bin"), os.path.join(d, "m.bin")
+        _write_csr(g, off, cols)
+        subprocess.run([REF_GPU_EXE, "slpa", g, str(niter), f"{int(T)},{int(seed)}", tr, mem], check=True,
+                       capture_output=True, timeout=600)
+        return (np.fromfile(tr, dtype=np.int32).reshape(niter, n),
+                np.ascontiguousarray(np.fromfile(mem, dtype=np.int32).reshape(n, T).T))

@@ -117,3 +117,31 @@ def test_summary_entry_points_reject_null_args():
     rounds = (C.c_int32 * 1)()
     rc = lib.glp_graph_fa_summary(None, labels, 0, verts, 1, 8, 0, keys, vals, rounds)
     assert rc == _lib.GLP_EINVAL and b"required" in lib.glp_last_error()
+
+
+def test_public_hooks_header_builds_a_user_hook_set(tmp_path):
+    """include/glp_hooks.cuh compiles with a hook set of the user's own and
+    links against the engine library (nvcc cross-compiles without a GPU)."""
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "hooks.cu"
+    src.write_text(r'''
+#include "glp_hooks.cuh"
+struct Halves {
+  glp_hooks::State st;
+  __device__ void pick(int32_t v) const { st.L[v] = st.Lnext[v]; }
+  __device__ void load(int32_t, int32_t sid, int64_t, int32_t* l, double* f) const { *l = st.L[sid]; *f = 0.5; }
+  __device__ double score(int32_t, int32_t l, double f) const { return f - 1e-9 * l; }
+  __device__ void update(int32_t, int32_t, double) const {}
+};
+extern "C" int run_halves(glp_graph* g, int32_t niter, int32_t* out) {
+  return glp_hooks::run(g, [](const glp_hooks::State& s) { return Halves{s}; }, niter, out, 0, nullptr, nullptr);
+}
+''')
+    so = tmp_path / "libhalves.so"
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-shared", "-Xcompiler",
+                    "-fPIC", "-I", os.path.join(root, "include"), str(src), "-o", str(so), "-L",
+                    os.path.join(root, "glp_b200"), "-lglp_b200"], check=True, timeout=600)
+    assert so.exists()

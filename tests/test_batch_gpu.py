@@ -7,6 +7,8 @@ runs.  Graphs cover every tier of the batch kernel (thread, warp, block),
 isolated vertices, single-vertex and edgeless graphs, and rows that are not
 strictly ascending (which turns the first-step closed form off).
 """
+import time
+
 import numpy as np
 import pytest
 import torch
@@ -86,7 +88,7 @@ def test_batch_every_configuration_agrees():
             for tt in (8, 16, 32):
                 for mid in (32, 64):
                     p = make_params(tiny_max=tt, mid_max=mid)
-                    p.reserved[0] = nt
+                    p.batch_threads = nt
                     lab, ch = b.run(8, p)
                     np.testing.assert_array_equal(lab, ref, err_msg=f"{nt} {tt} {mid}")
                     np.testing.assert_array_equal(ch, ref_ch)
@@ -98,7 +100,7 @@ def test_batch_tune_graph_replay_and_device_labels():
         ref, ref_ch = b.run(12)
         best, times = b.tune(2)
         assert len(times) == 12 and (times > 0).any()
-        assert best.tiny_max in (8, 16, 32) and best.mid_max in (32, 64) and best.reserved[0] in (512, 1024)
+        assert best.tiny_max in (8, 16, 32) and best.mid_max in (32, 64) and best.batch_threads in (512, 1024)
         lab, ch = b.run(12)
         np.testing.assert_array_equal(lab, ref)
         p = make_params(use_graph=1)
@@ -185,3 +187,27 @@ def test_batch_repack_reuses_the_object():
             for g in subset:
                 np.testing.assert_array_equal(lab[base:base + g.n], _solo(g, k)[0])
                 base += g.n
+
+
+def test_batch_barrier_timeout_is_reported_and_the_batch_stays_usable():
+    """Failure path of the persistent kernel's grid barrier, without a GPU
+    fault: one block withholds its arrival at the first barrier
+    (fault_skip_cta), so every block's bounded wait (50 ms here) runs out;
+    the run returns GLP_ETIMEOUT, and later runs on the same batch are
+    correct."""
+    gs = _mixed()
+    with Batch(gs) as b:
+        ref, ref_ch = b.run(6)
+        p = make_params(barrier_limit_us=50000, fault_skip_cta=1)
+        t0 = time.perf_counter()
+        with pytest.raises(_lib.GlpError) as e:
+            b.run(6, p)
+        assert e.value.code == _lib.GLP_ETIMEOUT
+        assert time.perf_counter() - t0 < 4.0  # the 50 ms limit, not the 5 s default
+        lab, ch = b.run(6)
+        np.testing.assert_array_equal(lab, ref)
+        np.testing.assert_array_equal(ch, ref_ch)
+        # the same short limit with every block arriving changes nothing
+        lab, ch = b.run(6, make_params(barrier_limit_us=50000))
+        np.testing.assert_array_equal(lab, ref)
+        np.testing.assert_array_equal(ch, ref_ch)

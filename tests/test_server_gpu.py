@@ -171,3 +171,81 @@ def test_resident_graphs_serve_many_requests():
         assert st["status"] == 0
     # small classic requests on resident graphs ride the batched rounds
     assert any(st["path"] == 1 for st in sts)
+
+
+def _long_layered():
+    # several hundred milliseconds on one B200: room to cancel it mid-run
+    return graphs.rmat(18, 16, seed=131), _lib.METHOD_LAYERED, 200, make_params(dstar=[2, 3, 5, 9, 17])
+
+
+def test_cancel_before_admission_and_before_start():
+    """Host-side failure handling: a tiny budget keeps requests pending; a
+    cancelled pending request ends with GLP_ECANCELED without running, and
+    the others still give their solo results."""
+    big, m, k, p = _long_layered()
+    small = [graphs.planted(20000, 8, 10.0, 2.0, seed=140 + i) for i in range(4)]
+    # the server's device-byte estimate of a one-graph solve on a host CSR:
+    # CSR + labels, volumes, plan and lists (48 B a vertex) + hub scratch
+    # (8 B an edge) + 64 MiB; a budget of 1.5 of it admits one such solve
+    est = 4 * (big.n + 1) + 4 * (big.m + 4) + 48 * big.n + 8 * big.m + (64 << 20)
+    with Server(hbm_budget_bytes=int(1.5 * est), plain_workers=1) as s:
+        h_big = s.submit(big, m, k, p)
+        h_big2 = s.submit(big, m, k, p)  # does not fit beside the first: pending, FIFO head
+        hs = [s.submit(g, _lib.METHOD_CLASSIC, 10) for g in small]  # pending behind it
+        assert s.info()["pending"] >= 5
+        s.cancel(hs[1])
+        with pytest.raises(_lib.GlpError) as e:
+            s.wait(hs[1], 60000)
+        assert e.value.code == _lib.GLP_ECANCELED
+        rc, st = s.stats(hs[1])
+        assert rc == _lib.GLP_ECANCELED and st["start_s"] == 0.0  # it never ran
+        s.cancel(h_big2)  # the pending head: the requests behind it move on
+        with pytest.raises(_lib.GlpError) as e:
+            s.wait(h_big2, 60000)
+        assert e.value.code == _lib.GLP_ECANCELED
+        s.wait(h_big, 120000)
+        np.testing.assert_array_equal(h_big.labels, _solo(big, m, k, p))
+        for i in (0, 2, 3):
+            s.wait(hs[i], 120000)
+            np.testing.assert_array_equal(hs[i].labels, _solo(small[i], _lib.METHOD_CLASSIC, 10))
+        assert s.info()["in_flight"] == 0 and s.info()["used_bytes"] == 0
+
+
+def test_cancel_stops_a_running_solve_and_the_server_goes_on():
+    big, m, k, p = _long_layered()
+    with Server(plain_workers=1) as s:
+        gid = s.add_graph(big)
+        h = s.submit_graph(gid, m, k, p)
+        t0 = time.perf_counter()
+        while s.stats(h)[1]["start_s"] == 0.0 and time.perf_counter() - t0 < 30:
+            time.sleep(0.001)
+        with pytest.raises(_lib.GlpError) as e:
+            s.wait(h, 1)  # a 1 ms wait on a running solve runs out
+        assert e.value.code == _lib.GLP_ETIMEOUT
+        s.cancel(h)
+        with pytest.raises(_lib.GlpError) as e:
+            s.wait(h, 60000)
+        assert e.value.code == _lib.GLP_ECANCELED
+        # the same resident graph serves the next request normally
+        h2 = s.submit_graph(gid, _lib.METHOD_CLASSIC, 10)
+        s.wait(h2, 60000)
+        np.testing.assert_array_equal(h2.labels, _solo(big, _lib.METHOD_CLASSIC, 10))
+        s.cancel(h2)  # already finished: its result stands
+        assert s.stats(h2)[0] == 0
+
+
+def test_cancel_flag_on_a_graph_handle():
+    """glp_graph_set_cancel_flag: a set flag stops glp_run at the next
+    iteration boundary with GLP_ECANCELED; cleared, the handle runs on."""
+    import ctypes as C
+    g = graphs.rmat(14, 16, seed=150)
+    flag = C.c_int32(1)
+    with Graph(g) as h:
+        lib = _lib.load()
+        _lib.check(lib.glp_graph_set_cancel_flag(h._h, C.byref(flag)))
+        with pytest.raises(_lib.GlpError) as e:
+            h.run(_lib.METHOD_CLASSIC, 10)
+        assert e.value.code == _lib.GLP_ECANCELED
+        flag.value = 0
+        np.testing.assert_array_equal(h.run(_lib.METHOD_CLASSIC, 10).labels, _solo(g, _lib.METHOD_CLASSIC, 10))
+        _lib.check(lib.glp_graph_set_cancel_flag(h._h, None))
