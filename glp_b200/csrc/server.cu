@@ -191,16 +191,18 @@ void admit_locked(glp_server* s) {
 
 bool idle_locked(const glp_server* s) { return s->stopping && s->pending.empty() && s->in_flight == 0; }
 
-void plain_worker(glp_server* s) {
-  cudaSetDevice(s->cfg.device);
-  // one handle per resident graph this worker has served: plans and buffers
-  // are built once and reused by later requests on that graph
+// One-graph solves with a handle per resident graph: plans and buffers are
+// built once and reused by later requests on that graph.  Each worker thread
+// owns one.
+struct OneGraphRunner {
   struct Cached {
     glp_graph* g;
     int64_t bytes;
   };
+  glp_server* s;
   std::unordered_map<int64_t, Cached> cache;
-  auto drop = [&](int64_t id) {
+
+  void drop(int64_t id) {
     auto it = cache.find(id);
     if (it == cache.end()) return;
     glp_graph_destroy(it->second.g);
@@ -209,35 +211,24 @@ void plain_worker(glp_server* s) {
       s->used_bytes -= it->second.bytes;
     }
     cache.erase(it);
-  };
-  for (;;) {
-    Request* r = nullptr;
-    std::vector<int64_t> stale;
-    {
-      std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_work.wait(lk, [&] { return !s->plain_q.empty() || idle_locked(s); });
-      for (auto& kv : cache)
-        if (s->removed_graphs.count(kv.first)) stale.push_back(kv.first);
-      if (s->plain_q.empty()) {
-        lk.unlock();
-        for (auto& kv : cache) {
-          glp_graph_destroy(kv.second.g);
-          std::lock_guard<std::mutex> lk2(s->mu);
-          s->used_bytes -= kv.second.bytes;
-        }
-        return;
-      }
-      // shortest expected job first, aged by its wait so none starves
-      const double now = s->now();
-      auto best = s->plain_q.begin();
-      for (auto it = s->plain_q.begin(); it != s->plain_q.end(); ++it)
-        if ((*it)->cost_s - (now - (*it)->stats.admit_s) < (*best)->cost_s - (now - (*best)->stats.admit_s)) best = it;
-      r = *best;
-      s->plain_q.erase(best);
-      r->stats.start_s = now;
-      r->stats.path = 0;
+  }
+  // Caller holds s->mu: handles of removed graphs to drop outside the lock.
+  std::vector<int64_t> stale_locked() const {
+    std::vector<int64_t> out;
+    for (auto& kv : cache)
+      if (s->removed_graphs.count(kv.first)) out.push_back(kv.first);
+    return out;
+  }
+  void clear() {
+    for (auto& kv : cache) {
+      glp_graph_destroy(kv.second.g);
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->used_bytes -= kv.second.bytes;
     }
-    for (int64_t id : stale) drop(id);
+    cache.clear();
+  }
+  // Solves r with glp_run and finishes it.
+  void run(Request* r) {
     glp_graph* g = nullptr;
     bool transient = true;
     int rc = GLP_OK;
@@ -272,6 +263,36 @@ void plain_worker(glp_server* s) {
     const std::string err = rc ? glp_last_error() : std::string();
     if (transient) glp_graph_destroy(g);
     finish(s, r, rc, rc ? err.c_str() : nullptr);
+  }
+};
+
+void plain_worker(glp_server* s) {
+  cudaSetDevice(s->cfg.device);
+  OneGraphRunner one{s, {}};
+  for (;;) {
+    Request* r = nullptr;
+    std::vector<int64_t> stale;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return !s->plain_q.empty() || idle_locked(s); });
+      stale = one.stale_locked();
+      if (s->plain_q.empty()) {
+        lk.unlock();
+        one.clear();
+        return;
+      }
+      // shortest expected job first, aged by its wait so none starves
+      const double now = s->now();
+      auto best = s->plain_q.begin();
+      for (auto it = s->plain_q.begin(); it != s->plain_q.end(); ++it)
+        if ((*it)->cost_s - (now - (*it)->stats.admit_s) < (*best)->cost_s - (now - (*best)->stats.admit_s)) best = it;
+      r = *best;
+      s->plain_q.erase(best);
+      r->stats.start_s = now;
+      r->stats.path = 0;
+    }
+    for (int64_t id : stale) one.drop(id);
+    one.run(r);
     {
       std::lock_guard<std::mutex> lk(s->mu);
       admit_locked(s);
@@ -287,14 +308,22 @@ void batch_worker(glp_server* s) {
   cudaStream_t up = nullptr;  // uploads of host CSRs, finished before packing
   cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
   glp_batch* b = nullptr;     // kept across rounds: repacking reuses its buffers
+  // A round of one request runs as a one-graph solve: the persistent kernel
+  // is a cooperative launch that needs every SM free, so alone it would wait
+  // for whatever else occupies the GPU and gain nothing from batching.
+  OneGraphRunner one{s, {}};
   for (;;) {
     std::vector<Request*> round;
+    std::vector<int64_t> stale;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       s->cv_work.wait(lk, [&] { return !s->batch_q.empty() || idle_locked(s); });
+      stale = one.stale_locked();
       if (s->batch_q.empty()) {
+        lk.unlock();
         if (up) cudaStreamDestroy(up);
         glp_batch_destroy(b);
+        one.clear();
         return;
       }
       while (!s->batch_q.empty() && (int32_t)round.size() < s->cfg.max_batch_graphs) {
@@ -304,9 +333,20 @@ void batch_worker(glp_server* s) {
       const double t = s->now();
       for (Request* r : round) {
         r->stats.start_s = t;
-        r->stats.path = 1;
+        r->stats.path = round.size() > 1 ? 1 : 0;
         r->stats.batch_graphs = (int32_t)round.size();
       }
+    }
+    for (int64_t id : stale) one.drop(id);
+    if (round.size() == 1) {
+      one.run(round[0]);
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        admit_locked(s);
+      }
+      s->cv_done.notify_all();
+      s->cv_work.notify_all();
+      continue;
     }
     // pack in order of iteration count (the batch wants them non-decreasing);
     // host CSRs are uploaded first so the whole round packs device to device
