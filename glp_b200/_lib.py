@@ -22,7 +22,7 @@ GLP_ECANCELED = -7
 GLP_EKERNEL = -8
 GLP_EAGAIN = -9
 
-METHOD_CLASSIC, METHOD_LAYERED, METHOD_SLPA, METHOD_USER = 1, 2, 3, 4
+METHOD_CLASSIC, METHOD_LAYERED, METHOD_SLPA, METHOD_USER, METHOD_SEEDED = 1, 2, 3, 4, 5
 BACKEND_EXACT, BACKEND_CM, BACKEND_FA = 0, 1, 2
 HOOKS_CLASSIC, HOOKS_LAYERED, HOOKS_WEIGHTED_DEGREE = 0, 1, 2
 GRAPH_SYMMETRIC = 1
@@ -100,6 +100,7 @@ SIGNATURES = {
     "glp_graph_check": (C.c_int, [C.c_void_p]),
     "glp_graph_device_view": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "glp_graph_set_cancel_flag": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "glp_graph_set_seeds": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "glp_graph_cm_sketch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                                       C.c_void_p]),
     "glp_graph_fa_summary": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,

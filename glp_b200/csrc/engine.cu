@@ -22,6 +22,7 @@
 
 #include "engine.h"
 #include "hooks_engine.cuh"
+#include "seeded.cuh"
 #include "smem_attr.h"
 
 namespace glp {
@@ -1195,6 +1196,35 @@ static int run_hooks(RunCtx& c, const glp_params& p, int32_t niter) {
 }
 
 
+// --------------------------------------------------------------- method 5
+// Seeded LP (prop/seedLprop.cuh): seeds fixed at their ids, every other
+// vertex starts unlabelled and takes the mode of its labelled neighbours.
+template <bool W>
+static int run_seeded(RunCtx& c, int32_t niter) {
+  glp_graph* g = c.g;
+  if (!g->d_seeds) {
+    set_error("method 5 needs seeds: call glp_graph_set_seeds first");
+    return GLP_EINVAL;
+  }
+  if (g->max_degree > kSeedSmem / 2 && !g->d_seed_keys) {
+    GLP_CUDA(dev_alloc(&g->d_seed_keys, sizeof(uint32_t) * 2 * (size_t)g->m));
+    GLP_CUDA(dev_alloc(&g->d_seed_vals, sizeof(uint32_t) * 2 * (size_t)g->m));
+  }
+  k_seeded_init<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(g->d_seeds, g->d_lab[0], g->d_lab[1], g->n);
+  ++c.launches;
+  const unsigned grid = (unsigned)std::min<int64_t>(cdiv(g->n, 8), (int64_t)device_sms() * 16);
+  int rc;
+  for (int32_t it = 0; it < niter; ++it) {
+    k_seeded_step<W><<<grid, 256, 0, c.s>>>(g->d_off, g->d_cols, g->d_w, g->d_seeds, g->d_lab[it & 1],
+                                            g->d_lab[(it + 1) & 1], g->n, g->d_seed_keys, g->d_seed_vals,
+                                            g->d_changed + it, g->d_err);
+    ++c.launches;
+    GLP_CUDA(cudaGetLastError());
+    if ((rc = after_iter(c, it, g->d_lab[(it + 1) & 1]))) return rc;
+  }
+  return GLP_OK;
+}
+
 // ------------------------------------------------- allocation-free classic LP
 // Scratch of glp_run_classic_noalloc: one copy per device (module globals are
 // per context), found with cudaGetSymbolAddress.
@@ -1368,6 +1398,9 @@ void glp_graph_destroy(glp_graph* g) {
   dev_free(g->d_err);
   dev_free(g->d_hook_keys);
   dev_free(g->d_hook_vals);
+  dev_free(g->d_seeds);
+  dev_free(g->d_seed_keys);
+  dev_free(g->d_seed_vals);
   if (g->stream) cudaStreamDestroy(g->stream);
   for (cudaStream_t st : g->aux)
     if (st) cudaStreamDestroy(st);
@@ -1444,6 +1477,28 @@ int glp_graph_check(glp_graph* g) {
   }
   if (!g->d_err) return GLP_OK;
   return check_err(g, g->stream);
+}
+
+int glp_graph_set_seeds(glp_graph* g, const uint8_t* seeds, int32_t on_device) {
+  if (!g) {
+    set_error("graph is NULL");
+    return GLP_EINVAL;
+  }
+  GLP_CUDA(cudaSetDevice(g->device));
+  int rc;
+  if ((rc = quiesce(g))) return rc;
+  if (!seeds) {
+    if (g->d_seeds) dev_free(g->d_seeds);
+    g->d_seeds = nullptr;
+    return GLP_OK;
+  }
+  if (!g->d_seeds) GLP_CUDA(dev_alloc(&g->d_seeds, std::max<size_t>((size_t)g->n, 1)));
+  if (g->n) {
+    GLP_CUDA(cudaMemcpyAsync(g->d_seeds, seeds, (size_t)g->n,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, g->stream));
+    GLP_CUDA(cudaStreamSynchronize(g->stream));
+  }
+  return GLP_OK;
 }
 
 int glp_graph_set_cancel_flag(glp_graph* g, const volatile int32_t* flag) {
@@ -1649,8 +1704,14 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
       }
       if (p.hooks == GLP_HOOKS_LAYERED) total = p.nlayers * niter;
       break;
+    case GLP_METHOD_SEEDED:
+      if (!g->d_seeds) {
+        set_error("method 5 needs seeds: call glp_graph_set_seeds first");
+        return GLP_EINVAL;
+      }
+      break;
     default:
-      set_error("method %d not in 1..4", method);
+      set_error("method %d not in 1..5", method);
       return GLP_ENOTSUP;
   }
   if (p.backend != GLP_BACKEND_EXACT && p.backend != GLP_BACKEND_CM && p.backend != GLP_BACKEND_FA) {
@@ -1698,6 +1759,10 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
       break;
     case GLP_METHOD_USER:
       rc = run_hooks(c, p, niter);
+      break;
+    case GLP_METHOD_SEEDED:
+      rc = W ? run_seeded<true>(c, niter) : run_seeded<false>(c, niter);
+      c.iter_base = niter & 1;
       break;
   }
   if (rc) return rc;

@@ -135,6 +135,10 @@ struct glp_graph {
   // method-4 spill tables (2 slots per CSR entry), allocated on first use
   uint32_t* d_hook_keys = nullptr;
   double* d_hook_vals = nullptr;
+  // method 5: seed flags (glp_graph_set_seeds) and integer spill tables
+  uint8_t* d_seeds = nullptr;
+  uint32_t* d_seed_keys = nullptr;
+  uint32_t* d_seed_vals = nullptr;
   int symmetric = -1;    // -1 unknown, 0 no, 1 yes (every edge stored both ways)
   int rows_sorted = -1;  // -1 unknown, 0 no, 1 every row strictly ascending
   int deg_sorted = 0;    // 1: degrees never increase along the vertex ids

@@ -162,6 +162,17 @@ class Graph:
     def check(self) -> None:
         _lib.check(self._lib.glp_graph_check(self._h))
 
+    def set_seeds(self, seeds) -> None:
+        """Seed vertices of method 5 (a boolean / 0-1 array of n entries; None
+        clears them)."""
+        if seeds is None:
+            _lib.check(self._lib.glp_graph_set_seeds(self._h, None, 0))
+            return
+        s = np.ascontiguousarray(np.asarray(seeds) != 0, dtype=np.uint8)
+        if s.shape != (self.n,):
+            raise ValueError("seeds must hold n entries")
+        _lib.check(self._lib.glp_graph_set_seeds(self._h, C.c_void_p(s.ctypes.data), 0))
+
     def _inspect_args(self, labels, vertices):
         lab = np.ascontiguousarray(labels, dtype=np.int32)
         if lab.shape != (self.n,):
@@ -299,6 +310,21 @@ class SLPAprop(_Prop):
 class UserdefinedLprop(_Prop):
     """method 4, the PickLabel/LoadNeighbor/LabelScore/UpdateVertex hooks (README.md:72-101)."""
     METHOD = _lib.METHOD_USER
+
+
+class seedLprop(_Prop):
+    """method 5, seeded LP (prop/seedLprop.cuh): seeds keep their id label,
+    the others take the mode of their labelled neighbours."""
+    METHOD = _lib.METHOD_SEEDED
+
+    def __init__(self, G: CSRGraph | CSR, seeds, params: _lib.Params | None = None):
+        super().__init__(G, params)
+        self.seeds = seeds
+
+    def run(self, niter: int) -> Result:
+        with Graph(self.G) as g:
+            g.set_seeds(self.seeds)
+            return g.run(self.METHOD, niter, self.params)
 
 
 PROPAGATORS = {1: classicLprop, 2: MultiLprop, 3: SLPAprop, 4: UserdefinedLprop}

@@ -45,6 +45,7 @@ extern "C" {
 #define GLP_METHOD_LAYERED 2 /* prop/MultiLprop.cuh + tutorial/CPUlp.cuh:169-262 */
 #define GLP_METHOD_SLPA 3    /* prop/SLPAprop.cuh, semantics tutorial/Base5prop.cuh */
 #define GLP_METHOD_USER 4    /* prop/UserdefinedLprop.cuh + README.md:72-101 hooks */
+#define GLP_METHOD_SEEDED 5  /* prop/seedLprop.cuh: seeds fixed, glp_graph_set_seeds */
 
 /* ---- counting back-ends (method/hashtable.cuh, countmin.cuh, frequent.cuh)
  * Every back-end gives the same labels, bit for bit.  CM and FA change how
@@ -217,6 +218,16 @@ int glp_graph_cm_sketch(glp_graph* g, const int32_t* labels, int32_t labels_on_d
 int glp_graph_fa_summary(glp_graph* g, const int32_t* labels, int32_t labels_on_device, const int32_t* vertices,
                          int32_t nv, int32_t capacity, int32_t ref_compat, uint32_t* keys, uint32_t* vals,
                          int32_t* rounds);
+
+/* Seeds of method 5 (seeded LP; prop/seedLprop.cuh, whose seed list is read
+ * from a file, :161-181).  seeds[v] != 0 marks vertex v as a seed (n bytes,
+ * host or device); NULL clears them.  A method-5 run labels every seed with
+ * its own id and every other vertex -1 (unlabelled, as
+ * initialize_labels_by_seeds, header/kernel.cuh:453-466); then, every
+ * iteration, a seed keeps its label and any other vertex takes the label of
+ * largest count (weight sum) among its LABELLED neighbours, ties -> the
+ * largest label, keeping its own when none is labelled. */
+int glp_graph_set_seeds(glp_graph* g, const uint8_t* seeds, int32_t on_device);
 
 /* Cancellation of runs on this handle: while flag (host memory, NULL = none)
  * is non-zero, glp_run stops at the next iteration boundary with

@@ -454,6 +454,44 @@ int orc_fa_summary(int32_t v, const int32_t* off, const int32_t* cols, const int
   return rounds;
 }
 
+// Seeded LP (prop/seedLprop.cuh; seed kernels header/kernel.cuh:914-1031,
+// :1742-1836, :5236-5290; start labels initialize_labels_by_seeds, :453-466):
+// seeds start with their id and keep it; every other vertex starts at -1 and
+// takes, each synchronous step, the label of largest count (weight sum) among
+// its labelled (>= 0) neighbours, ties -> the largest label, keeping its own
+// label when none is labelled.  (The reference's tiers disagree on
+// unlabelled neighbours; this is the rule its big and huge kernels follow
+// for labelled ones.)  trace (nullable): labels after every step [niter][n].
+int orc_seeded_run(int32_t n, const int32_t* off, const int32_t* cols, const int32_t* w, const uint8_t* seeds,
+                   int32_t niter, int32_t* lout, int32_t* trace, int nthreads) {
+  const int nt = threads_or_default(nthreads);
+  std::vector<int32_t> a(n), b(n);
+  for (int32_t v = 0; v < n; ++v) a[v] = seeds[v] ? v : -1;
+  for (int32_t it = 0; it < niter; ++it) {
+#pragma omp parallel num_threads(nt)
+    {
+      std::vector<LW> buf;
+#pragma omp for schedule(dynamic, 1024)
+      for (int32_t v = 0; v < n; ++v) {
+        if (seeds[v]) {
+          b[v] = a[v];
+          continue;
+        }
+        buf.clear();
+        for (int32_t j = off[v]; j < off[v + 1]; ++j)
+          if (a[cols[j]] >= 0) buf.push_back({a[cols[j]], w ? (int64_t)w[j] : 1});
+        int32_t bl;
+        int64_t bc;
+        b[v] = mode_of(buf, &bl, &bc) ? bl : a[v];
+      }
+    }
+    std::swap(a, b);
+    if (trace) std::memcpy(trace + (size_t)it * n, a.data(), sizeof(int32_t) * n);
+  }
+  std::memcpy(lout, a.data(), sizeof(int32_t) * n);
+  return 0;
+}
+
 // ---------------------------------------------------------------- graphs
 // The seeded R-MAT workload built on the host, for the CPU legs of the
 // benchmark (which must not load the engine library) and to check the

@@ -53,6 +53,7 @@ def load():
     lib.orc_rmat_csr.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                  C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.c_int]
     lib.orc_free.argtypes = [vp]
+    lib.orc_seeded_run.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_int32, vp, vp, C.c_int]
     lib.orc_count_diff.restype = C.c_int64
     lib.orc_count_diff.argtypes = [C.c_int32, vp, vp]
     _lib = lib
@@ -126,6 +127,19 @@ def slpa_run(off, cols, T: int, niter: int, seed: int, r: float, w=None, threads
     if spoken:
         res["spoken"] = sp[:niter]
     return res
+
+
+def seeded_run(off, cols, seeds, niter: int, w=None, trace: bool = False, threads: int = 0):
+    """Seeded LP (seeds keep their id; the others take the mode of their
+    labelled neighbours); returns labels (and [niter][n] trace if asked)."""
+    off, cols, w = _csr(off, cols, w)
+    n = len(off) - 1
+    s = np.ascontiguousarray(np.asarray(seeds) != 0, dtype=np.uint8)
+    out = np.empty(n, dtype=np.int32)
+    tr = np.empty((max(niter, 1), n), dtype=np.int32) if trace else None
+    load().orc_seeded_run(n, _p(off), _p(cols), _p(w) if w is not None else None, _p(s), niter, _p(out),
+                          _p(tr) if trace else None, threads)
+    return (out, tr[:niter]) if trace else out
 
 
 def cpulp_sync_run_1(off, cols, niter: int):

@@ -169,3 +169,18 @@ def test_frequent_items_misra_gries_bound():
     for l in range(40):
         assert est.get(l, 0) <= counts[l]
         assert counts[l] - est.get(l, 0) <= rounds
+
+
+def test_seeded_known_answers():
+    """Seeded LP by hand: a path seeded at one end labels one more vertex per
+    step; an unseeded component stays unlabelled; a vertex between two seeds
+    of equal weight takes the larger seed id."""
+    from tests.graphs_fixtures import path, undirected
+    off, cols = path(5)
+    seeds = np.array([1, 0, 0, 0, 0], np.uint8)
+    _, tr = O.seeded_run(off, cols, seeds, 4, trace=True)
+    assert tr[0].tolist() == [0, 0, -1, -1, -1]
+    assert tr[3].tolist() == [0, 0, 0, 0, 0]
+    off, cols = undirected(6, [(0, 1), (1, 2), (3, 4)])
+    seeds = np.array([1, 0, 1, 0, 0, 0], np.uint8)
+    assert O.seeded_run(off, cols, seeds, 3).tolist() == [0, 2, 2, -1, -1, -1]
