@@ -26,6 +26,7 @@ METHOD_CLASSIC, METHOD_LAYERED, METHOD_SLPA, METHOD_USER, METHOD_SEEDED = 1, 2, 
 BACKEND_EXACT, BACKEND_CM, BACKEND_FA = 0, 1, 2
 HOOKS_CLASSIC, HOOKS_LAYERED, HOOKS_WEIGHTED_DEGREE = 0, 1, 2
 GRAPH_SYMMETRIC = 1
+EDGES_DIRECTED, EDGES_KEEP_IDS = 1, 2
 MAX_LAYERS = 32
 
 _ERRNAMES = {
@@ -101,6 +102,9 @@ SIGNATURES = {
     "glp_graph_device_view": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "glp_graph_set_cancel_flag": (C.c_int, [C.c_void_p, C.c_void_p]),
     "glp_graph_set_seeds": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "glp_graph_from_edges": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_uint32,
+                                       C.c_void_p, C.POINTER(C.c_void_p)]),
+    "glp_graph_export": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "glp_graph_cm_sketch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                                       C.c_void_p]),
     "glp_graph_fa_summary": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,
@@ -136,6 +140,8 @@ SIGNATURES = {
                                     C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int64)]),
     "glp_server_add_graph": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64,
                                        C.c_int32, C.POINTER(C.c_int64)]),
+    "glp_server_add_edges": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                                       C.c_uint32, C.c_void_p, C.POINTER(C.c_int64)]),
     "glp_server_submit_graph": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
                                           C.POINTER(C.c_int64)]),
     "glp_server_remove_graph": (C.c_int, [C.c_void_p, C.c_int64]),

@@ -25,7 +25,7 @@ ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle.so")
 
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp"]
-ENGINE_SOURCES = ["engine.cu", "graphgen.cu", "batch.cu", "server.cu"]
+ENGINE_SOURCES = ["engine.cu", "graphgen.cu", "batch.cu", "server.cu", "ingest.cu"]
 
 
 def _nvcc() -> str:

@@ -1410,6 +1410,21 @@ void glp_graph_destroy(glp_graph* g) {
   delete g;
 }
 
+int glp_graph_export(const glp_graph* g, int32_t* offsets, int32_t* cols, int32_t* weights, int32_t on_device) {
+  if (!g || !offsets || (g->m > 0 && !cols)) {
+    set_error("graph, offsets and cols are required");
+    return GLP_EINVAL;
+  }
+  GLP_CUDA(cudaSetDevice(g->device));
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  GLP_CUDA(cudaMemcpyAsync(offsets, g->d_off, sizeof(int32_t) * ((size_t)g->n + 1), k, g->stream));
+  if (g->m) GLP_CUDA(cudaMemcpyAsync(cols, g->d_cols, sizeof(int32_t) * (size_t)g->m, k, g->stream));
+  if (g->m && weights && g->d_w)
+    GLP_CUDA(cudaMemcpyAsync(weights, g->d_w, sizeof(int32_t) * (size_t)g->m, k, g->stream));
+  GLP_CUDA(cudaStreamSynchronize(g->stream));
+  return GLP_OK;
+}
+
 int glp_graph_info(const glp_graph* g, int32_t* n, int64_t* m, int32_t* max_degree) {
   if (!g) {
     set_error("graph is NULL");

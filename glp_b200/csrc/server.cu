@@ -46,6 +46,8 @@
 
 namespace glp {
 void set_error(const char* fmt, ...);
+int ingest_edges(const int32_t* src, const int32_t* dst, int64_t count, int32_t n, int32_t on_device, uint32_t flags,
+                 int32_t** d_off, int32_t** d_cols, int64_t* m, int32_t* d_old, cudaStream_t s);
 }  // namespace glp
 
 namespace {
@@ -603,6 +605,63 @@ int glp_server_add_graph(glp_server* s, const int32_t* offsets, const int32_t* c
     }
   g->max_degree = host_max_degree(hoff.data(), n);
   std::lock_guard<std::mutex> lk(s->mu);
+  g->id = s->next_graph++;
+  *graph_id = g->id;
+  s->graphs.emplace(g->id, std::move(g));
+  return GLP_OK;
+}
+
+int glp_server_add_edges(glp_server* s, const int32_t* src, const int32_t* dst, int64_t count, int32_t n,
+                         int32_t on_device, uint32_t flags, int32_t* old_id, int64_t* graph_id) {
+  if (!s || !graph_id) {
+    set_error("bad graph arguments");
+    return GLP_EINVAL;
+  }
+  // the CSR is built on the device; its size is known only afterwards, so the
+  // budget is checked against the edge count's bound first
+  const int64_t bound = 4 * ((int64_t)n + 1) + 4 * std::max<int64_t>(((flags & GLP_EDGES_DIRECTED) ? 1 : 2) * count, 1);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->used_bytes + bound > s->cfg.hbm_budget_bytes) {
+      set_error("adding the graph would exceed the server's HBM budget");
+      return GLP_ENOMEM;
+    }
+    s->used_bytes += bound;  // reserved while building
+  }
+  std::unique_ptr<Resident> g(new Resident());
+  cudaStream_t st = nullptr;
+  int rc = cudaSetDevice(s->cfg.device) == cudaSuccess && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) ==
+                                                                cudaSuccess
+               ? GLP_OK
+               : GLP_ECUDA;
+  int32_t* d_old = nullptr;
+  if (!rc && old_id) {
+    if (on_device) d_old = old_id;
+    else if (cudaMalloc(&d_old, sizeof(int32_t) * (size_t)std::max(n, 1)) != cudaSuccess) rc = GLP_ENOMEM;
+  }
+  if (!rc) rc = glp::ingest_edges(src, dst, count, n, on_device, flags, &g->d_off, &g->d_cols, &g->m, d_old, st);
+  if (!rc && old_id && !on_device &&
+      (cudaMemcpy(old_id, d_old, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess))
+    rc = GLP_ECUDA;
+  std::vector<int32_t> hoff;
+  if (!rc) {
+    hoff.resize((size_t)n + 1);
+    if (cudaMemcpy(hoff.data(), g->d_off, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = GLP_ECUDA;
+  }
+  if (old_id && !on_device && d_old) cudaFree(d_old);
+  if (st) cudaStreamDestroy(st);
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->used_bytes -= bound;
+  if (rc) {
+    free_resident(g.get());
+    if (rc == GLP_ECUDA) set_error("building the graph on the device failed");
+    return rc;
+  }
+  g->n = n;
+  g->bytes = 4 * (int64_t)(n + 1) + 4 * std::max<int64_t>(g->m, 1);
+  g->max_degree = host_max_degree(hoff.data(), n);
+  s->used_bytes += g->bytes;
   g->id = s->next_graph++;
   *graph_id = g->id;
   s->graphs.emplace(g->id, std::move(g));

@@ -126,6 +126,46 @@ class Graph:
                                                  C.byref(h)))
         self._h = h
 
+    @classmethod
+    def from_edges(cls, src, dst, n: int, directed: bool = False, keep_ids: bool = False):
+        """A graph built on the device from an edge list (glp_graph_from_edges):
+        self loops dropped, symmetrised unless `directed`, deduplicated,
+        renumbered by degree descending unless `keep_ids`.  src/dst: int32
+        tensors (host or CUDA) or arrays.  Returns (Graph, old_id) with old_id
+        the original id of each vertex (a numpy array)."""
+        src = torch.as_tensor(src, dtype=torch.int32).contiguous()
+        dst = torch.as_tensor(dst, dtype=torch.int32).contiguous()
+        if src.shape != dst.shape or src.dim() != 1:
+            raise ValueError("src and dst must be 1-D of equal length")
+        if dst.device != src.device:
+            dst = dst.to(src.device)
+        lib = _lib.load()
+        on_dev = 1 if src.device.type == "cuda" else 0
+        if on_dev:
+            torch.cuda.synchronize(src.device)
+        old = torch.empty(max(n, 1), dtype=torch.int32, device=src.device)
+        flags = (_lib.EDGES_DIRECTED if directed else 0) | (_lib.EDGES_KEEP_IDS if keep_ids else 0)
+        h = C.c_void_p()
+        _lib.check(lib.glp_graph_from_edges(C.c_void_p(src.data_ptr()) if src.numel() else None,
+                                            C.c_void_p(dst.data_ptr()) if dst.numel() else None,
+                                            C.c_int64(src.numel()), n, on_dev, flags, C.c_void_p(old.data_ptr()),
+                                            C.byref(h)))
+        self = cls.__new__(cls)
+        self._lib = lib
+        self._h = h
+        info = self.info()
+        self.n, self.m = info["n"], info["m"]
+        self.weighted = False
+        return self, old[:n].cpu().numpy()
+
+    def export(self) -> CSR:
+        """The handle's CSR as host tensors (glp_graph_export)."""
+        off = np.empty(self.n + 1, dtype=np.int32)
+        cols = np.empty(max(self.m, 1), dtype=np.int32)
+        _lib.check(self._lib.glp_graph_export(self._h, C.c_void_p(off.ctypes.data), C.c_void_p(cols.ctypes.data),
+                                              None, 0))
+        return from_numpy(off, cols[:self.m])
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.glp_graph_destroy(self._h)

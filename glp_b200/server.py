@@ -108,6 +108,25 @@ class Server:
         self._sizes[gid.value] = g.n
         return gid.value
 
+    def add_edges(self, src, dst, n: int, directed: bool = False, keep_ids: bool = False) -> tuple[int, np.ndarray]:
+        """Build a resident graph on the device from an edge list
+        (glp_server_add_edges); returns (graph id, original id of each vertex)."""
+        import torch
+        src = torch.as_tensor(src, dtype=torch.int32).contiguous()
+        dst = torch.as_tensor(dst, dtype=torch.int32).contiguous().to(src.device)
+        on_dev = 1 if src.device.type == "cuda" else 0
+        if on_dev:
+            torch.cuda.synchronize(src.device)
+        old = torch.empty(max(n, 1), dtype=torch.int32, device=src.device)
+        flags = (_lib.EDGES_DIRECTED if directed else 0) | (_lib.EDGES_KEEP_IDS if keep_ids else 0)
+        gid = C.c_int64()
+        _lib.check(self._lib.glp_server_add_edges(self._h, C.c_void_p(src.data_ptr()) if src.numel() else None,
+                                                  C.c_void_p(dst.data_ptr()) if dst.numel() else None,
+                                                  C.c_int64(src.numel()), n, on_dev, flags,
+                                                  C.c_void_p(old.data_ptr()), C.byref(gid)))
+        self._sizes[gid.value] = n
+        return gid.value, old[:n].cpu().numpy()
+
     def submit_graph(self, graph_id: int, method: int, niter: int, params: _lib.Params | None = None) -> Request:
         """Submit a solve on a resident graph; returns at once."""
         n = self._sizes[graph_id]

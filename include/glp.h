@@ -169,6 +169,23 @@ int glp_plan_offsets(const int32_t* offsets, int32_t n, const glp_params* p, int
 /* Reports (and clears) kernel error flags raised by asynchronous runs. */
 int glp_graph_check(glp_graph* g);
 
+/* Graph construction on the device from an edge list (count pairs
+ * src[i] -> dst[i], ids in [0, n); host or device arrays).  Replaces the
+ * reference's offline normaliser and loader (tools/normalize.cpp:262-348,
+ * header/graph.h:226-258): self loops dropped; unless GLP_EDGES_DIRECTED,
+ * every edge stored in both directions; duplicate entries dropped; unless
+ * GLP_EDGES_KEEP_IDS, vertices renumbered by degree descending, ties by the
+ * smaller original id; rows ascending.  old_id (nullable, n entries, host or
+ * device as the edges) receives the original id of each vertex.  count <
+ * 2^30. */
+#define GLP_EDGES_DIRECTED 1u
+#define GLP_EDGES_KEEP_IDS 2u
+int glp_graph_from_edges(const int32_t* src, const int32_t* dst, int64_t count, int32_t n, int32_t on_device,
+                         uint32_t flags, int32_t* old_id, glp_graph** out);
+/* Copies a handle's CSR out: offsets [n+1], cols [m], weights [m] (nullable;
+ * ignored for an unweighted graph), device pointers when on_device. */
+int glp_graph_export(const glp_graph* g, int32_t* offsets, int32_t* cols, int32_t* weights, int32_t on_device);
+
 /* Device view of a handle for method-4 hook sets compiled outside the
  * library (include/glp_hooks.cuh).  Replaces the reference's route for user
  * hooks -- editing the __device__ stubs of header/kernel.cuh:6071-6085 and
@@ -373,6 +390,11 @@ int glp_server_add_graph(glp_server* s, const int32_t* offsets, const int32_t* c
                          int64_t m, int32_t on_device, int64_t* graph_id);
 int glp_server_submit_graph(glp_server* s, int64_t graph_id, int32_t method, const glp_params* p, int32_t niter,
                             int32_t* labels_out, int64_t* id);
+/* A resident graph built on the device from an edge list, with the
+ * semantics and arguments of glp_graph_from_edges; requests on it go through
+ * glp_server_submit_graph. */
+int glp_server_add_edges(glp_server* s, const int32_t* src, const int32_t* dst, int64_t count, int32_t n,
+                         int32_t on_device, uint32_t flags, int32_t* old_id, int64_t* graph_id);
 int glp_server_remove_graph(glp_server* s, int64_t graph_id);
 /* GLP_EAGAIN while the request waits or runs; its status once done. */
 int glp_server_poll(glp_server* s, int64_t id, glp_request_stats* stats);
