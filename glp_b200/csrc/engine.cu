@@ -632,6 +632,7 @@ struct RunCtx {
   int iter_base = 0;
   int32_t backend = GLP_BACKEND_EXACT;  // counting back-end of the big tier
   bool serial = false;                  // glp_params.serial_step: one stream per step
+  int32_t merge_rounds = 1;             // glp_params.reserved[0]: merge rounds per counted chunk
 
   ~RunCtx() {
     for (auto& v : evs)
@@ -872,6 +873,7 @@ static int run_classic(RunCtx& c, int32_t niter) {
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_lab[it & 1], g->d_lab[it & 1], g->d_lab[(it + 1) & 1],
                g->d_changed + it, g->d_err, p.d_mode, g->n, fr ? p.chg[it & 1] : nullptr,
                fr ? p.counts + 7 + (it & 1) : nullptr};
+    a.merge_rounds = c.merge_rounds;
     if (fr) GLP_CUDA(cudaMemsetAsync(p.counts + 7 + (it & 1), 0, sizeof(uint32_t), c.s));
     StepLaunch L = c.launch();
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
@@ -924,6 +926,7 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       // term is looked up (from the previous step's changes within the layer)
       StepArgs a{g->d_off, g->d_cols, g->d_w, lin,     lin,   lout, g->d_changed + step, g->d_err,
                  g->plan.d_mode, g->n, nullptr, nullptr};
+      a.merge_rounds = c.merge_rounds;
       StepLaunch L = c.launch();
       L.prev_changed = it > 0 ? g->d_changed + step - 1 : nullptr;
       L.allow_majority = 0;
@@ -965,6 +968,7 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
     GLP_CUDA(cudaGetLastError());
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_spoken, lcur, lout, g->d_changed + it, g->d_err,
                g->plan.d_mode, g->n, nullptr, nullptr};
+    a.merge_rounds = c.merge_rounds;
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
     L.allow_majority = 1;  // the listener mode; spoken labels change every step: no frontier
     if (it == 0 && g->rows_sorted == 1) {
@@ -1755,6 +1759,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.user = cb_user;
   c.backend = p.backend;
   c.serial = p.serial_step != 0;
+  c.merge_rounds = p.reserved[0] >= 1 && p.reserved[0] <= 8 ? p.reserved[0] : 1;
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;
