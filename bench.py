@@ -328,7 +328,7 @@ def full_count_roofline(plan: dict, runs: list, n: int, peak: float) -> dict:
     full_steps = 0
     for r in runs:
         ch = r.changed
-        st = r.extra.get("step_tier_ms") if r.extra else None
+        st = r.step_tier_ms
         if st is None:
             continue
         for it in range(1, len(ch)):
@@ -423,10 +423,18 @@ def run_glp(args, ws, rank, local):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    parts = {"create_ms": 0.0, "run_ms": 0.0, "destroy_ms": 0.0}
     for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
         h2 = Graph(host_csr)
+        t1 = time.perf_counter()
         h2.run(_lib.METHOD_CLASSIC, args.iters, params, labels_out=lab_pin)
+        t2 = time.perf_counter()
         h2.close()
+        t3 = time.perf_counter()
+        parts["create_ms"] += (t1 - t0) * 1e3 / args.e2e_steps
+        parts["run_ms"] += (t2 - t1) * 1e3 / args.e2e_steps
+        parts["destroy_ms"] += (t3 - t2) * 1e3 / args.e2e_steps
     e1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
@@ -476,7 +484,8 @@ def run_glp(args, ws, rank, local):
             "step": f"one {args.iters}-iteration run over the device-resident graph",
             "parallelism": f"replicas{ws}", "graph_gen_s": round(gen_s, 2),
             "e2e": {"value": round(e2e_value, 3), "unit": "GTEPS", "h2d_bytes_per_step": int(4 * (n + 1 + m)),
-                    "d2h_bytes_per_step": int(4 * n), "steps": args.e2e_steps, "labels_match_device_run": same},
+                    "d2h_bytes_per_step": int(4 * n), "steps": args.e2e_steps, "labels_match_device_run": same,
+                    "host_clock_parts": {k: round(v, 2) for k, v in parts.items()}},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": roof.get("achieved"), "peak": peak, "unit": "GB/s",
                          "frac": roof.get("frac"), "traffic": traffic, "kernel": roof.get("kernel"),
@@ -651,14 +660,16 @@ def run_served(args, ws, rank, local):
                   "batched_frac": round(sum(st["path"] == 1 for st in stats) / len(stats), 3)}
         # sequential one-request-at-a-time engine, same schedule, the same
         # graphs resident (one handle each, created before the stream)
-        lat_s, same = [], True
+        lat_s, same, service = [], True, []
         resident = [Graph(g) for g in pool]
         start = time.perf_counter()
         for r, at, h in zip(reqs, arrivals, handles):
             wait = start + at - time.perf_counter()
             if wait > 0:
                 time.sleep(wait)
+            t_run = time.perf_counter()
             lab = resident[r["gi"]].run(r["method"], r["niter"], r["params"]).labels
+            service.append(time.perf_counter() - t_run)
             lat_s.append((time.perf_counter() - (start + at)) * 1e3)
             same = same and bool(np.array_equal(lab, h.labels))
         span_s = (time.perf_counter() - start)
@@ -666,9 +677,26 @@ def run_served(args, ws, rank, local):
             gh.close()
         seq = {"throughput": round(len(reqs) / span_s, 1), "p50_ms": round(_pct(lat_s, 50), 2),
                "p99_ms": round(_pct(lat_s, 99), 2)}
+        # where the sequential engine's time goes, per request class: the
+        # served speed-up this mix can reach is bounded by the classes that
+        # batching does not shorten
+        classes = {}
+        for r, t in zip(reqs, service):
+            key = ("planted" if r["g"].n <= 100000 else "rmat") + "-" + {1: "classic", 2: "layered", 3: "slpa"}[
+                r["method"]]
+            c = classes.setdefault(key, {"requests": 0, "service_s": 0.0})
+            c["requests"] += 1
+            c["service_s"] += t
+        total_s = sum(service)
+        for c in classes.values():
+            c["mean_ms"] = round(1e3 * c["service_s"] / c["requests"], 3)
+            c["share"] = round(c["service_s"] / total_s, 4)
+            c["service_s"] = round(c["service_s"], 3)
+        unbatched = sum(c["service_s"] for k, c in classes.items() if k != "planted-classic")
         out.append({"rate": rate, "served": served, "sequential": seq,
                     "throughput_vs_sequential": round(served["throughput"] / seq["throughput"], 2),
-                    "labels_match_alone": same})
+                    "labels_match_alone": same, "sequential_service_by_class": classes,
+                    "bound_if_batched_classes_were_free": round(total_s / max(unbatched, 1e-9), 2)})
     mix = {"planted": round(sum(r["g"].n <= 100000 for r in reqs) / len(reqs), 3),
            "classic": round(sum(r["method"] == 1 for r in reqs) / len(reqs), 3),
            "layered": round(sum(r["method"] == 2 for r in reqs) / len(reqs), 3),
