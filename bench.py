@@ -453,7 +453,7 @@ def run_glp(args, ws, rank, local):
     total_bytes_iter = 8 * m + 12 * n + 4
     iter_ms = ms / (args.steps * args.iters)
 
-    cpu, parity = None, None
+    cpu, parity, refgpu = None, None, None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         off_np, cols_np = off_h.numpy(), cols_h.numpy()
         try:
@@ -461,6 +461,29 @@ def run_glp(args, ws, rank, local):
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GTEPS", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+        # the reference's own GPU kernels (header/kernel.cuh's five classic bin
+        # kernels, driven by oracle/_ref/ref_gpu_lp with a correct plan) on
+        # the same graph and GPU: device time of the same 20 iterations
+        refgpu = None
+        exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_lp")
+        if os.path.exists(exe):
+            try:
+                with tempfile.TemporaryDirectory() as d:
+                    path, lab_path = os.path.join(d, "g.csr"), os.path.join(d, "l.bin")
+                    write_csr(path, off_np, cols_np)
+                    r = subprocess.run([exe, "classic-time", path, str(args.iters), "-", lab_path],
+                                       capture_output=True, text=True, check=True, timeout=900)
+                    total = float(re.search(r"total_ms ([0-9.eE+-]+)", r.stdout).group(1))
+                    ref_lab = np.fromfile(lab_path, dtype=np.int32)
+                refgpu = {"value": round(m * args.iters / (total / 1e3) / 1e9, 3), "unit": "GTEPS",
+                          "ms_per_run": round(total, 3),
+                          "labels_differing_from_this_engine": int(np.count_nonzero(ref_lab != dev_labels)),
+                          "what": "the reference's own classic bin kernels (header/kernel.cuh l_*_labelload, "
+                                  "its thresholds and launch shapes) on this GPU, one run of the same iterations, "
+                                  "CUDA events per step; labels differ where its medium/big lanes break ties "
+                                  "differently"}
+            except Exception as e:
+                refgpu = {"value": None, "what": f"failed: {e}"}
         # parity of the headline run's final labels with the oracle (the
         # synchronous rule restated on the CPU), outside every timed region
         try:
@@ -502,6 +525,7 @@ def run_glp(args, ws, rank, local):
             "plan": plan,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "reference_gpu_kernels": refgpu,
             "parity": parity,
         }
     handle.close()

@@ -37,6 +37,7 @@
 //
 // usage:
 //   ref_gpu_lp classic <graph.csr> <niter> <init.bin|-> <trace.bin>
+//   ref_gpu_lp classic-time <graph.csr> <niter> - <labels.bin>   (prints per-step device ms)
 //   ref_gpu_lp layered <graph.csr> <niter> <dstar,dstar,...> <trace.bin> [<vol.bin>]
 //   ref_gpu_lp slpa    <graph.csr> <niter> <T,seed> <trace.bin> <memory.bin>
 // graph.csr: int64 n, int64 m, int32 offsets[n+1], int32 cols[m].
@@ -369,7 +370,27 @@ int main(int argc, char** argv) {
   Dev d = upload(g, p);
   FILE* tr = std::fopen(argv[5], "wb");
   if (!tr) die("cannot open the trace file");
-  if (mode == "classic") {
+  if (mode == "classic-time") {
+    // device time of each synchronous step (the reference's per-iteration
+    // work: label copy, table and hub-maxima clears, the five bin kernels),
+    // CUDA events around the step, no label dump inside the timed span
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double total = 0;
+    for (int it = 0; it < niter; ++it) {
+      CK(cudaEventRecord(e0));
+      classic_step(g, p, d);
+      CK(cudaEventRecord(e1));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      total += ms;
+      std::printf("iter %d ms %.4f\n", it, ms);
+    }
+    std::printf("total_ms %.4f\n", total);
+    dump(tr, d.lw, g.n);
+  } else if (mode == "classic") {
     if (std::strcmp(argv[4], "-") != 0) {
       std::vector<int32_t> init((size_t)g.n);
       FILE* f = std::fopen(argv[4], "rb");

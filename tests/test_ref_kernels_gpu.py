@@ -187,3 +187,23 @@ def test_ref_slpa_memory_equals_oracle_and_engine():
             res = h.run(_lib.METHOD_SLPA, niter, make_params(slpa_T=T, slpa_r=0.1, seed=seed), slpa_outputs=True)
         np.testing.assert_array_equal(res.slpa_mem, ref_mem)
         np.testing.assert_array_equal(res.labels, ref_tr[-1])
+
+
+def test_ref_classic_timing_mode_runs_the_same_steps():
+    """classic-time (the benchmark's reference-kernel baseline) runs the same
+    steps as classic: equal final labels, a positive device time per step."""
+    import re
+    import subprocess
+    import tempfile
+    g = graphs.rmat(14, 16, seed=3, device="cpu")
+    off, cols, _ = g.numpy()
+    want = O.ref_gpu_classic(off, cols, 6)[-1]
+    with tempfile.TemporaryDirectory() as d:
+        path, lab = os.path.join(d, "g.csr"), os.path.join(d, "l.bin")
+        O._write_csr(path, off, cols)
+        r = subprocess.run([O.REF_GPU_EXE, "classic-time", path, "6", "-", lab], capture_output=True, text=True,
+                           check=True, timeout=600)
+        got = np.fromfile(lab, dtype=np.int32)
+    times = [float(x) for x in re.findall(r"iter \d+ ms ([0-9.]+)", r.stdout)]
+    assert len(times) == 6 and all(t > 0 for t in times)
+    np.testing.assert_array_equal(got, want)
