@@ -63,7 +63,10 @@ class Params(C.Structure):
         ("batch_threads", C.c_int32),
         ("barrier_limit_us", C.c_int32),
         ("fault_skip_cta", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("majority_permille", C.c_int32),
+        ("frontier_permille", C.c_int32),
+        ("l2_window", C.c_int32),
+        ("reserved", C.c_int32 * 1),
         ("serial_step", C.c_int32),
     ]
 

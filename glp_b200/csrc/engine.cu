@@ -442,7 +442,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   if (modal) {
     GLP_CUDA(cudaMemsetAsync(p.counts, 0, 7 * sizeof(uint32_t), s));
     k_step_mode<<<1, 1, 0, s>>>(L.prev_changed, a.n, a.n - (int32_t)p.isolated, L.allow_majority,
-                                L.allow_frontier, p.d_mode);
+                                L.allow_frontier, L.majority_pm, L.frontier_pm, p.d_mode);
     ++*launches;
     if (L.allow_frontier && L.front.chg_in) {
       const unsigned fgrid = device_sms() * 16;
@@ -632,7 +632,8 @@ struct RunCtx {
   int iter_base = 0;
   int32_t backend = GLP_BACKEND_EXACT;  // counting back-end of the big tier
   bool serial = false;                  // glp_params.serial_step: one stream per step
-  int32_t merge_rounds = 1;             // glp_params.reserved[0]: merge rounds per counted chunk
+  uint32_t majority_pm = 250, frontier_pm = 50;  // glp_params step-mode thresholds
+  bool l2_window = false;               // glp_params.l2_window
 
   ~RunCtx() {
     for (auto& v : evs)
@@ -671,6 +672,8 @@ struct RunCtx {
     StepLaunch L{&g->plan, s, ev, {g->aux[0], g->aux[1]}, g->fork, {g->join[0], g->join[1]}};
     L.backend = backend;
     L.serial = serial;
+    L.majority_pm = majority_pm;
+    L.frontier_pm = frontier_pm;
     return L;
   }
   cudaEvent_t* current() { return timing && used ? evs[used - 1].data() : nullptr; }
@@ -862,18 +865,49 @@ static int ensure_symmetric(glp_graph* g) {
   return GLP_OK;
 }
 
+// glp_params.l2_window: the label array a step gathers from is kept in L2
+// through a persisting access-policy window on the run's three streams (the
+// persisting set-aside is a limit of this process's context; it is released
+// when the run ends).  lab = nullptr clears the window.
+static void set_l2_window(RunCtx& c, const int32_t* lab) {
+  if (!c.l2_window) return;
+  glp_graph* g = c.g;
+  int max_win = 0, max_persist = 0;
+  if (cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, g->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, g->device) != cudaSuccess ||
+      max_win <= 0 || max_persist <= 0) {
+    cudaGetLastError();
+    return;
+  }
+  cudaStreamAttrValue v{};
+  if (lab) {
+    const size_t bytes = std::min<size_t>((size_t)g->n * sizeof(int32_t), (size_t)max_win);
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)max_persist);
+    v.accessPolicyWindow.base_ptr = const_cast<int32_t*>(lab);
+    v.accessPolicyWindow.num_bytes = bytes;
+    v.accessPolicyWindow.hitRatio = std::min(1.0f, (float)max_persist / (float)std::max<size_t>(bytes, 1));
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  } else {
+    v.accessPolicyWindow.num_bytes = 0;
+  }
+  for (cudaStream_t st : {c.s, g->aux[0], g->aux[1]}) cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v);
+  if (!lab) cudaCtxResetPersistingL2Cache();
+  cudaGetLastError();
+}
+
 template <bool W>
 static int run_classic(RunCtx& c, int32_t niter) {
   glp_graph* g = c.g;
   int rc = init_labels(c);
   if (rc) return rc;
   for (int32_t it = 0; it < niter; ++it) {
+    set_l2_window(c, g->d_lab[it & 1]);
     const bool fr = g->symmetric == 1;
     DevicePlan& p = g->plan;
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_lab[it & 1], g->d_lab[it & 1], g->d_lab[(it + 1) & 1],
                g->d_changed + it, g->d_err, p.d_mode, g->n, fr ? p.chg[it & 1] : nullptr,
                fr ? p.counts + 7 + (it & 1) : nullptr};
-    a.merge_rounds = c.merge_rounds;
     if (fr) GLP_CUDA(cudaMemsetAsync(p.counts + 7 + (it & 1), 0, sizeof(uint32_t), c.s));
     StepLaunch L = c.launch();
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
@@ -922,12 +956,12 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       }
       int32_t* lin = g->d_lab[it & 1];
       int32_t* lout = g->d_lab[(it + 1) & 1];
+      set_l2_window(c, lin);
       // full counting every step; the step mode only chooses how the volume
       // term is looked up (from the previous step's changes within the layer)
       StepArgs a{g->d_off, g->d_cols, g->d_w, lin,     lin,   lout, g->d_changed + step, g->d_err,
                  g->plan.d_mode, g->n, nullptr, nullptr};
-      a.merge_rounds = c.merge_rounds;
-      StepLaunch L = c.launch();
+        StepLaunch L = c.launch();
       L.prev_changed = it > 0 ? g->d_changed + step - 1 : nullptr;
       L.allow_majority = 0;
       L.allow_frontier = 0;
@@ -957,6 +991,7 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
   if (!g->d_spoken) GLP_CUDA(dev_alloc(&g->d_spoken, sizeof(int32_t) * std::max(g->n, 1)));
   GLP_CUDA(cudaMemsetAsync(g->d_mem, 0xff, sizeof(int32_t) * (size_t)T * g->n, c.s));
   if ((rc = init_labels(c))) return rc;
+  set_l2_window(c, g->d_spoken);
   for (int32_t it = 0; it < niter; ++it) {
     int32_t* lcur = g->d_lab[it & 1];
     int32_t* lout = g->d_lab[(it + 1) & 1];
@@ -968,7 +1003,6 @@ static int run_slpa(RunCtx& c, const glp_params& p, int32_t niter, glp_outputs* 
     GLP_CUDA(cudaGetLastError());
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_spoken, lcur, lout, g->d_changed + it, g->d_err,
                g->plan.d_mode, g->n, nullptr, nullptr};
-    a.merge_rounds = c.merge_rounds;
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
     L.allow_majority = 1;  // the listener mode; spoken labels change every step: no frontier
     if (it == 0 && g->rows_sorted == 1) {
@@ -1759,7 +1793,9 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.user = cb_user;
   c.backend = p.backend;
   c.serial = p.serial_step != 0;
-  c.merge_rounds = p.reserved[0] >= 1 && p.reserved[0] <= 8 ? p.reserved[0] : 1;
+  if (p.majority_permille > 0) c.majority_pm = (uint32_t)std::min(p.majority_permille, 1000);
+  if (p.frontier_permille > 0) c.frontier_pm = (uint32_t)std::min(p.frontier_permille, 1000);
+  c.l2_window = p.l2_window != 0;
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;
@@ -1785,6 +1821,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
       c.iter_base = niter & 1;
       break;
   }
+  set_l2_window(c, nullptr);
   if (rc) return rc;
   const int32_t* final_lab = g->d_lab[c.iter_base];
   if (g->n)

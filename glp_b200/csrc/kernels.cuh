@@ -46,10 +46,6 @@ struct StepArgs {
   // vertices whose label changed this step are appended here (nullable)
   int32_t* chg_out;
   uint32_t* chg_out_n;
-  // exact-count kernels: lanes of a 32-entry chunk that hold the same label
-  // as the first not-yet-merged lane are merged into one insert, this many
-  // rounds per chunk (1: the label of lane 0 only)
-  int32_t merge_rounds = 1;
 };
 
 // Counts (and, when a.chg_out is set, lists) the vertices whose label changed.
@@ -125,12 +121,12 @@ __device__ __forceinline__ bool use_majority(const StepArgs& a) { return step_mo
 // few distinct labels); 0 = score at every insert, the lookup issued before
 // the insert so that its latency overlaps the hashing.
 __global__ void k_step_mode(const unsigned long long* prev_changed, int32_t n, int32_t n_active, int allow_majority,
-                            int allow_frontier, int32_t* mode) {
+                            int allow_frontier, uint32_t majority_pm, uint32_t frontier_pm, int32_t* mode) {
   int32_t m = kModeFull, scan = 0;
   if (prev_changed) {
     const unsigned long long c = *prev_changed;
-    if (allow_frontier && c * 20ull < (unsigned long long)n) m = kModeFrontier;
-    else if (allow_majority && c * 4ull < (unsigned long long)n) m = kModeMajority;
+    if (allow_frontier && c * 1000ull < (unsigned long long)frontier_pm * (unsigned long long)n) m = kModeFrontier;
+    else if (allow_majority && c * 1000ull < (unsigned long long)majority_pm * (unsigned long long)n) m = kModeMajority;
     scan = c * 2ull < (unsigned long long)n_active ? 1 : 0;
   }
   mode[0] = m;
@@ -356,23 +352,15 @@ __global__ void __launch_bounds__(256) k_group(StepArgs a, TierWork tw, S score)
 // lanes of the warp.
 template <bool W, class S, class Ins>
 __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, const S& score, const Ins& insert,
-                                            Best& best, bool& fail, bool scan = false, int rounds = 1) {
+                                            Best& best, bool& fail, bool scan = false) {
   const int lane = threadIdx.x & 31;
+  const int32_t l0 = __shfl_sync(kFull, has ? lab : -1, 0);
+  const uint32_t m0 = __ballot_sync(kFull, has && lab == l0);
   uint32_t k = W ? wt : 1u;
-  // merge rounds: the first lane still unmerged counts every lane holding its
-  // label (a hot label of a forming community costs one atomic per chunk
-  // instead of one per lane, since equal-address shared atomics serialise)
-  uint32_t pending = __ballot_sync(kFull, has);
-#pragma unroll 1
-  for (int r = 0; r < rounds && pending; ++r) {
-    const int lead = __ffs(pending) - 1;
-    const int32_t lr = __shfl_sync(kFull, lab, lead);
-    const bool same = has && lab == lr;
-    const uint32_t mr = __ballot_sync(kFull, same);
-    const uint32_t kr = W ? __reduce_add_sync(kFull, same ? wt : 0u) : (uint32_t)__popc(mr);
-    if (lane == lead) k = kr;
-    else if (same) has = false;  // counted by the lead lane
-    pending &= ~mr;
+  if (l0 >= 0) {
+    const uint32_t k0 = W ? __reduce_add_sync(kFull, lab == l0 && has ? wt : 0u) : (uint32_t)__popc(m0);
+    if (lane == 0) k = k0;
+    else if (has && lab == l0) has = false;  // counted by lane 0
   }
   if (!has) return;
   const int32_t vl = (S::kScan && !scan) ? score.vol_of(lab) : 0;  // in flight during the insert
@@ -517,7 +505,7 @@ __global__ void __launch_bounds__(NT, S::kPacked ? (C16 ? 2048 : 1536) / NT : 10
         if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + 32 * q < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, a.merge_rounds);
+        if (j0 + 32 * q < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
     }
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {
@@ -644,7 +632,7 @@ __global__ void __launch_bounds__(NT, (S::kPacked && !W) ? 2048 / NT : (S::kPack
         if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + q * NT < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, a.merge_rounds);
+        if (j0 + q * NT < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
     }
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {  // block-uniform

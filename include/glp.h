@@ -103,7 +103,14 @@ typedef struct glp_params {
   int32_t fault_skip_cta;         /* glp_batch_run, for tests of the failure path: 1 + the index of a
                                      block that never arrives at the first grid barrier, so that the
                                      other blocks' bounded waits run out (0 = off) */
-  int32_t reserved[4];
+  int32_t majority_permille;      /* classic / SLPA steps after the first: below this many changes per
+                                     1000 vertices in the previous step, a step first decides the vertices
+                                     whose own label holds a strict majority (0 = 250); every mode is exact */
+  int32_t frontier_permille;      /* below this many changes per 1000 vertices, only neighbours of changed
+                                     vertices are recomputed (symmetric graphs; 0 = 50) */
+  int32_t l2_window;              /* 1: keep the label array being gathered in L2 through a persisting
+                                     access-policy window on the run's streams (off by default) */
+  int32_t reserved[1];
   int32_t serial_step;            /* 1: every kernel of a step runs on the run's own
                                      stream instead of three forked streams, so that
                                      the per-tier event times of glp_outputs are each

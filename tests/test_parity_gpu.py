@@ -386,3 +386,21 @@ def test_classic_oscillation_per_iteration(niter):
         r2 = h.run(_lib.METHOD_CLASSIC, niter)  # no per-iteration host sync
         np.testing.assert_array_equal(r2.labels, otr[-1])
         np.testing.assert_array_equal(r2.changed, ref_changed)
+
+
+@pytest.mark.parametrize("maj,fr,l2", [(1000, 50, 0), (250, 300, 0), (0, 0, 1), (1000, 1000, 1), (1, 1, 0)])
+def test_step_mode_thresholds_and_l2_window_keep_labels(maj, fr, l2):
+    """Every step mode is exact, so moving the thresholds between full,
+    majority and frontier steps, or keeping the gathered labels in L2, leaves
+    every iteration's labels (and change counts) unchanged."""
+    off, cols = CASES["rmat14"]
+    niter = 10
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, niter, majority_permille=maj, frontier_permille=fr,
+                         l2_window=l2)
+    _, otr = O.classic_run(off, cols, niter, trace=True)
+    for it in range(niter):
+        np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
+    lab, vol = O.layered_run(off, cols, [2, 5], 3)
+    with Graph(from_numpy(off, cols)) as h:
+        r = h.run(_lib.METHOD_LAYERED, 3, make_params(dstar=[2, 5], l2_window=l2))
+    np.testing.assert_array_equal(r.labels, lab)
