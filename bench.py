@@ -70,9 +70,11 @@ def parse():
     ap.add_argument("--iters", type=int, default=ITERS)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="classic", choices=["classic", "batched", "served"],
+    ap.add_argument("--workload", default="classic",
+                    choices=["classic", "batched", "served", "layered", "weighted", "slpa"],
                     help="classic: the R-MAT headline line (with a batched summary unless --no-batched); "
-                         "batched: the batched workload alone")
+                         "batched / served: that workload alone; layered / weighted / slpa: one run of that path "
+                         "on R-MAT --scale (SLPA: the overlapping planted graph of 2M vertices), for profiling")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the layered / weighted / SLPA measurements")
@@ -610,6 +612,42 @@ def run_suite(args, ws, rank, local):
             "how": "device time (CUDA events) of 2 runs after 1 warm-up run, graph resident, labels on the device"}
 
 
+def run_one_path(args, ws, rank, local):
+    """One path of the suite on its own (profiling): layered LP (5 layers x 3
+    iterations, dstar 2,3,5,9,17) or weighted classic LP (20 iterations) on
+    R-MAT --scale, or SLPA (T = 20, 20 iterations) on the overlapping planted
+    graph of 2M vertices; --warmup runs, then --steps runs timed with CUDA
+    events."""
+    from glp_b200 import _lib, graphs
+    from glp_b200.engine import Graph, make_params
+
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    if args.workload == "slpa":
+        g = graphs.overlapping(2_000_000, 2000, 0.1, 24.0, seed=4, device=dev)
+        method, niter, params, per_iter = _lib.METHOD_SLPA, 20, make_params(slpa_T=20, slpa_r=0.1, seed=4), 20
+    elif args.workload == "layered":
+        g = graphs.rmat(args.scale, 16, seed=args.seed, device=dev)
+        method, niter, params, per_iter = _lib.METHOD_LAYERED, 3, make_params(dstar=[2, 3, 5, 9, 17]), 15
+    else:
+        g = graphs.rmat(args.scale, 16, seed=args.seed, device=dev, weighted=True)
+        method, niter, params, per_iter = _lib.METHOD_CLASSIC, args.iters, make_params(), args.iters
+    stream = torch.cuda.current_stream(dev)
+    with Graph(g) as h:
+        lab = torch.empty(g.n, dtype=torch.int32, device=dev)
+        for _ in range(max(args.warmup, 1)):
+            h.run(method, niter, params, labels_out=lab, stream=stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            h.run(method, niter, params, labels_out=lab, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    return {"workload": args.workload, "n": g.n, "m": g.m, "ms_per_run": round(ms, 3),
+            "gteps_per_iter": round(g.m * per_iter / (ms / 1e3) / 1e9, 2)}
+
+
 # ----------------------------------------------------------------- served
 def served_requests(count: int, seed: int, device):
     """The served workload (seed 6): a pool of graphs (24 planted-partition
@@ -884,6 +922,10 @@ def main():
             print(json.dumps(res))
     elif args.workload == "served":
         res = run_served(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(res))
+    elif args.workload in ("layered", "weighted", "slpa"):
+        res = run_one_path(args, ws, rank, local)
         if rank == 0:
             print(json.dumps(res))
     else:
