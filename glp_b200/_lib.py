@@ -66,7 +66,7 @@ class Params(C.Structure):
         ("majority_permille", C.c_int32),
         ("frontier_permille", C.c_int32),
         ("l2_window", C.c_int32),
-        ("reserved", C.c_int32 * 1),
+        ("cycle_stop", C.c_int32),
         ("serial_step", C.c_int32),
     ]
 

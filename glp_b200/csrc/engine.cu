@@ -331,11 +331,14 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
       (rc = zeroed(&p, std::max<size_t>((size_t)n_big, 1), &p.fscreen.ids)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.front.act)) ||
       (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[0])) ||
-      (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[1]))) {
+      (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.chg[1])) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.cyc_old)) ||
+      (rc = zeroed(&p, std::max<size_t>((size_t)g->n, 1), &p.cyc_stamp)) || (rc = zeroed(&p, 1, &p.cyc_mism))) {
     free_plan(&p);
     return rc;
   }
   g->epoch = 0;  // fresh marks
+  g->cyc_tag = 0;
   p.fmid.count = p.counts;
   p.fbig.count = p.counts + 1;
   p.fscreen.count = p.counts + 9;
@@ -634,6 +637,8 @@ struct RunCtx {
   bool serial = false;                  // glp_params.serial_step: one stream per step
   uint32_t majority_pm = 250, frontier_pm = 50;  // glp_params step-mode thresholds
   bool l2_window = false;               // glp_params.l2_window
+  bool cycle = false;                   // stop a classic run once it ends in a two-step cycle
+  int32_t cycle_from = -1;              // first iteration not run (the labels repeat from there)
 
   ~RunCtx() {
     for (auto& v : evs)
@@ -896,11 +901,29 @@ static void set_l2_window(RunCtx& c, const int32_t* lab) {
   cudaGetLastError();
 }
 
+// Host-mapped verdict words and events of the two-step cycle detection.
+static int ensure_cycle_state(glp_graph* g) {
+  if (g->h_cycle) return GLP_OK;
+  GLP_CUDA(cudaHostAlloc(&g->h_cycle, 4 * sizeof(uint32_t), cudaHostAllocMapped));
+  GLP_CUDA(cudaHostGetDevicePointer(&g->d_cycle, g->h_cycle, 0));
+  for (cudaEvent_t& e : g->cyc_ev) GLP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return GLP_OK;
+}
+
 template <bool W>
 static int run_classic(RunCtx& c, int32_t niter) {
   glp_graph* g = c.g;
   int rc = init_labels(c);
   if (rc) return rc;
+  // two-step cycle detection: symmetric graphs (their change lists are kept),
+  // synchronous runs (the host reads the verdicts)
+  const bool track = c.cycle && g->symmetric == 1 && niter > 2;
+  if (track) {
+    if ((rc = ensure_cycle_state(g))) return rc;
+    for (int k = 0; k < 4; ++k) g->h_cycle[k] = 0u;
+  }
+  const uint32_t cyc_cap = (uint32_t)std::max<int64_t>(1024, g->n / 8);
+  const unsigned cyc_grid = (unsigned)device_sms() * 4;
   for (int32_t it = 0; it < niter; ++it) {
     set_l2_window(c, g->d_lab[it & 1]);
     const bool fr = g->symmetric == 1;
@@ -919,6 +942,14 @@ static int run_classic(RunCtx& c, int32_t niter) {
       L.front.chg_in = p.chg[(it - 1) & 1];
       L.front.chg_in_n = p.counts + 7 + ((it - 1) & 1);
     }
+    const uint32_t tag = ++g->cyc_tag;
+    if (track && it >= 1) {
+      // before the step overwrites them: L_{it-1} of the vertices step it-1 changed
+      GLP_CUDA(cudaMemsetAsync(p.cyc_mism, 0, sizeof(uint32_t), c.s));
+      k_cycle_save<<<cyc_grid, 256, 0, c.s>>>(p.chg[(it - 1) & 1], p.counts + 7 + ((it - 1) & 1), cyc_cap,
+                                             g->d_lab[(it + 1) & 1], p.cyc_old, p.cyc_stamp, tag, p.cyc_mism);
+      ++c.launches;
+    }
     if (it == 0 && g->rows_sorted == 1) {
       if (c.timing) {  // first_step takes the step's events itself
         c.used--;
@@ -928,7 +959,32 @@ static int run_classic(RunCtx& c, int32_t niter) {
     } else if ((rc = launch_step<W>(L, a, ScoreClassic{}, &c.launches))) {
       return rc;
     }
+    if (track && it >= 1) {
+      k_cycle_check<<<cyc_grid, 256, 0, c.s>>>(p.chg[it & 1], p.counts + 7 + (it & 1), p.counts + 7 + ((it - 1) & 1),
+                                              cyc_cap, g->d_lab[(it + 1) & 1], p.cyc_old, p.cyc_stamp, tag,
+                                              p.cyc_mism);
+      k_cycle_verdict<<<1, 1, 0, c.s>>>(p.cyc_mism, g->d_cycle + (it & 3));
+      c.launches += 2;
+      GLP_CUDA(cudaGetLastError());
+      GLP_CUDA(cudaEventRecord(g->cyc_ev[it % 3], c.s));
+    }
     if ((rc = after_iter(c, it, g->d_lab[(it + 1) & 1]))) return rc;
+    // the host stays at most two steps ahead: step it-1's verdict is read
+    // while step it runs; once a step ended in the cycle, the steps already
+    // enqueued are correct and the rest repeat the last two labelings
+    if (track && it >= 2) {
+      GLP_CUDA(cudaEventSynchronize(g->cyc_ev[(it - 1) % 3]));
+      if (*(volatile uint32_t*)(g->h_cycle + ((it - 1) & 3))) {
+        c.cycle_from = it + 1;
+        break;
+      }
+    }
+  }
+  if (c.cycle_from > 0) {
+    // L_t = L_{t-2} from here on, and L_t sits in buffer t & 1 already: the
+    // final labels need no copy; per-iteration observers see both buffers in turn
+    for (int32_t t = c.cycle_from; t < niter; ++t)
+      if ((rc = after_iter(c, t, g->d_lab[(t + 1) & 1]))) return rc;
   }
   return GLP_OK;
 }
@@ -1439,6 +1495,9 @@ void glp_graph_destroy(glp_graph* g) {
   dev_free(g->d_seeds);
   dev_free(g->d_seed_keys);
   dev_free(g->d_seed_vals);
+  if (g->h_cycle) cudaFreeHost(g->h_cycle);
+  for (cudaEvent_t e : g->cyc_ev)
+    if (e) cudaEventDestroy(e);
   if (g->stream) cudaStreamDestroy(g->stream);
   for (cudaStream_t st : g->aux)
     if (st) cudaStreamDestroy(st);
@@ -1796,6 +1855,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   if (p.majority_permille > 0) c.majority_pm = (uint32_t)std::min(p.majority_permille, 1000);
   if (p.frontier_permille > 0) c.frontier_pm = (uint32_t)std::min(p.frontier_permille, 1000);
   c.l2_window = p.l2_window != 0;
+  c.cycle = !p.async && p.cycle_stop == 0;
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;
@@ -1837,6 +1897,9 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
     GLP_CUDA(cudaMemcpyAsync(tmp.data(), g->d_changed, sizeof(unsigned long long) * total, cudaMemcpyDeviceToHost,
                              c.s));
     GLP_CUDA(cudaStreamSynchronize(c.s));
+    // iterations after a detected two-step cycle change what the last one did
+    if (c.cycle_from > 0)
+      for (int32_t i = c.cycle_from; i < total; ++i) tmp[i] = tmp[c.cycle_from - 1];
     for (int32_t i = 0; i < total; ++i) out->changed[i] = (int64_t)tmp[i];
   }
   if (out->tier_ms) {

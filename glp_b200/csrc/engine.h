@@ -82,6 +82,11 @@ struct DevicePlan {
   int32_t* chg[2] = {nullptr, nullptr};
   Frontier front{};
   int32_t* d_mode = nullptr;
+  // two-step cycle detection (classic, symmetric): labels before the last
+  // change, their step tags, and a mismatch word
+  int32_t* cyc_old = nullptr;
+  uint32_t* cyc_stamp = nullptr;
+  uint32_t* cyc_mism = nullptr;
   bool mid_c16 = true;  // mid counts fit 16 bits (unweighted, or small weight sums)
   int32_t n_hubs = 0, n_chunks = 0;
   int64_t isolated = 0;
@@ -147,6 +152,12 @@ struct glp_graph {
   cudaStream_t last_stream = nullptr;  // the stream of the latest run
   const volatile int32_t* cancel = nullptr;  // glp_graph_set_cancel_flag: non-zero stops a run
   uint32_t epoch = 0;  // frontier mark of the last step
+  // two-step cycle detection: host-mapped verdict words (a ring of 4 steps),
+  // their device alias, per-step events and the step tag
+  uint32_t* h_cycle = nullptr;
+  uint32_t* d_cycle = nullptr;
+  cudaEvent_t cyc_ev[3] = {nullptr, nullptr, nullptr};
+  uint32_t cyc_tag = 0;
   // auxiliary streams and fork/join events of a step
   cudaStream_t aux[2] = {nullptr, nullptr};
   cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};

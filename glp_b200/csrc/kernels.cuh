@@ -938,6 +938,54 @@ __global__ void k_hub_finalize(StepArgs a, HubPlan hp) {
   if (l != a.lcur[v]) record_change(a, v);
 }
 
+// ------------------------------------------------- two-step cycle detection
+// Synchronous LP on a symmetric graph often ends in a cycle of two labelings
+// (L_{t+1} = L_{t-1} for every vertex): a few vertices flip between two
+// labels for ever.  Once a step ends in that cycle every later labeling is
+// known exactly, so a run can stop there.  With S_t the vertices step t
+// changes (L_{t+1}(v) != L_t(v)), L_{t+1} = L_{t-1} holds iff S_t = S_{t-1}
+// and every v in S_t returns to L_{t-1}(v).  k_cycle_save keeps L_{t-1}(v)
+// for v in S_{t-1} before step t overwrites it; k_cycle_check compares after
+// the step; k_cycle_verdict publishes the answer to the host.  The lists are
+// walked only while they are short (at most `cap` entries); a longer list
+// marks the step as not cyclic.
+__global__ void k_cycle_save(const int32_t* __restrict__ chg_prev, const uint32_t* n_prev, uint32_t cap,
+                             const int32_t* __restrict__ lab_prev2, int32_t* __restrict__ old,
+                             uint32_t* __restrict__ stamp, uint32_t tag, uint32_t* mism) {
+  const uint32_t c = *n_prev;
+  if (c > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(mism, 1u);
+    return;
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+    const int32_t v = chg_prev[i];
+    old[v] = lab_prev2[v];
+    stamp[v] = tag;
+  }
+}
+
+__global__ void k_cycle_check(const int32_t* __restrict__ chg, const uint32_t* n_now, const uint32_t* n_prev,
+                              uint32_t cap, const int32_t* __restrict__ lab_next, const int32_t* __restrict__ old,
+                              const uint32_t* __restrict__ stamp, uint32_t tag, uint32_t* mism) {
+  const uint32_t c = *n_now;
+  if (c != *n_prev || c > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(mism, 1u);
+    return;
+  }
+  bool bad = false;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+    const int32_t v = chg[i];
+    bad |= stamp[v] != tag || lab_next[v] != old[v];
+  }
+  if (__any_sync(kFull, bad) && (threadIdx.x & 31) == 0) atomicOr(mism, 1u);
+}
+
+// flag: host-mapped word; 1 = the step ended in a two-step cycle.
+__global__ void k_cycle_verdict(const uint32_t* mism, volatile uint32_t* flag) {
+  *flag = *mism == 0u ? 1u : 0u;
+  __threadfence_system();
+}
+
 // ------------------------------------------------------- first-step shortcut
 // Before the first step every label is its vertex id.  When every row lists
 // strictly ascending columns (no repeated neighbour), every neighbour label

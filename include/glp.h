@@ -110,7 +110,11 @@ typedef struct glp_params {
                                      vertices are recomputed (symmetric graphs; 0 = 50) */
   int32_t l2_window;              /* 1: keep the label array being gathered in L2 through a persisting
                                      access-policy window on the run's streams (off by default) */
-  int32_t reserved[1];
+  int32_t cycle_stop;             /* classic runs on symmetric graphs: 0 (default) stops running steps
+                                     once a step ends in a two-step cycle (L_{t+1} = L_{t-1} for every
+                                     vertex), after which every labeling is known: the results and the
+                                     per-iteration outputs are those of all niter steps; -1 runs every
+                                     step */
   int32_t serial_step;            /* 1: every kernel of a step runs on the run's own
                                      stream instead of three forked streams, so that
                                      the per-tier event times of glp_outputs are each

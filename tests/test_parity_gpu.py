@@ -404,3 +404,26 @@ def test_step_mode_thresholds_and_l2_window_keep_labels(maj, fr, l2):
     with Graph(from_numpy(off, cols)) as h:
         r = h.run(_lib.METHOD_LAYERED, 3, make_params(dstar=[2, 5], l2_window=l2))
     np.testing.assert_array_equal(r.labels, lab)
+
+
+@pytest.mark.parametrize("scale", [14, 16])
+def test_two_step_cycle_stop_is_exact(scale):
+    """A classic run that ends in a two-step cycle stops running steps there;
+    its labels after every iteration, final labels and change counts equal
+    a run of every step (cycle_stop = -1) and the oracle's, while it launches
+    fewer kernels."""
+    off, cols, _ = rmat_np(scale, seed=2)
+    niter = 20
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, niter)
+    full, ftr = _run_trace(off, cols, _lib.METHOD_CLASSIC, niter, cycle_stop=-1)
+    _, otr = O.classic_run(off, cols, niter, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+    np.testing.assert_array_equal(ftr, otr)
+    np.testing.assert_array_equal(res.changed, full.changed)
+    g = graphs.from_numpy(off, cols)
+    with Graph(g, symmetric=True) as h:
+        a = h.run(_lib.METHOD_CLASSIC, niter)
+        b = h.run(_lib.METHOD_CLASSIC, niter, make_params(cycle_stop=-1))
+    np.testing.assert_array_equal(a.labels, otr[-1])
+    np.testing.assert_array_equal(a.changed, b.changed)
+    assert a.launches < b.launches
