@@ -635,7 +635,7 @@ struct RunCtx {
   int iter_base = 0;
   int32_t backend = GLP_BACKEND_EXACT;  // counting back-end of the big tier
   bool serial = false;                  // glp_params.serial_step: one stream per step
-  uint32_t majority_pm = 250, frontier_pm = 50;  // glp_params step-mode thresholds
+  uint32_t majority_pm = 500, frontier_pm = 50;  // glp_params step-mode thresholds
   bool l2_window = false;               // glp_params.l2_window
   bool cycle = false;                   // stop a classic run once it ends in a two-step cycle
   int32_t cycle_from = -1;              // first iteration not run (the labels repeat from there)

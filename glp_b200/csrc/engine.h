@@ -110,7 +110,7 @@ struct StepLaunch {
   Frontier front{};  // this step's frontier inputs (front.chg_in set from the second step)
   int32_t backend = GLP_BACKEND_EXACT;  // GLP_BACKEND_CM / _FA: summary screen on the big tier
   bool serial = false;  // every kernel on `stream` (per-tier timing without overlap)
-  uint32_t majority_pm = 250, frontier_pm = 50;  // step-mode thresholds (changes per 1000 vertices)
+  uint32_t majority_pm = 500, frontier_pm = 50;  // step-mode thresholds (changes per 1000 vertices)
 };
 
 template <bool W, class S>

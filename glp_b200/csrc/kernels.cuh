@@ -113,8 +113,9 @@ enum : int32_t { kModeFull = 0, kModeMajority = 1, kModeFrontier = 2 };
 __device__ __forceinline__ int32_t step_mode(const StepArgs& a) { return a.mode ? *a.mode : kModeFull; }
 __device__ __forceinline__ bool use_majority(const StepArgs& a) { return step_mode(a) == kModeMajority; }
 
-// Picks the mode from the previous step's changed count: frontier below n/20
-// changes (when allowed), majority below n/4 (when allowed), else full.
+// Picks the mode from the previous step's changed count: frontier below
+// frontier_pm changes per 1000 vertices (default 50), majority below
+// majority_pm (default 500), when the method allows them; else full.
 // mode[1] (scores that need a per-label lookup, layered LP): 1 = score each
 // distinct label once from the finished table, worth it once fewer than half
 // of the n_active non-isolated vertices changed (their neighbourhoods hold

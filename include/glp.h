@@ -105,7 +105,7 @@ typedef struct glp_params {
                                      other blocks' bounded waits run out (0 = off) */
   int32_t majority_permille;      /* classic / SLPA steps after the first: below this many changes per
                                      1000 vertices in the previous step, a step first decides the vertices
-                                     whose own label holds a strict majority (0 = 250); every mode is exact */
+                                     whose own label holds a strict majority (0 = 500); every mode is exact */
   int32_t frontier_permille;      /* below this many changes per 1000 vertices, only neighbours of changed
                                      vertices are recomputed (symmetric graphs; 0 = 50) */
   int32_t l2_window;              /* 1: keep the label array being gathered in L2 through a persisting
