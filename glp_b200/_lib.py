@@ -68,6 +68,8 @@ class Params(C.Structure):
         ("l2_window", C.c_int32),
         ("cycle_stop", C.c_int32),
         ("serial_step", C.c_int32),
+        ("mid_prefetch", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 

@@ -534,19 +534,35 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       const TierWork tw{vs, none, none, 1};
       const size_t smr = 4ull * kBigPartMax[r] * sizeof(uint32_t);
       const unsigned grid = (unsigned)std::min<int64_t>(vs.n, kMaxGrid);
+      // unweighted classic: each warp's first round of the next vertex is in
+      // flight while the current one is counted (L.mid_prefetch)
+      constexpr bool pf_ok = !W && S::kPacked;
+      const bool pf = pf_ok && L.mid_prefetch;
       if (k16 && r > 0 && r < kBigParts - 1) {
         const size_t sm16 = 12ull * kBigPartMax[r];  // 2*max slots of 4 + 2 bytes
         if (r == 1) {
-          k_big<256, false, S, true><<<grid, 256, sm16, s>>>(a, tw, score);
+          if (pf) k_big<256, false, S, true, pf_ok><<<grid, 256, sm16, s>>>(a, tw, score);
+          else k_big<256, false, S, true><<<grid, 256, sm16, s>>>(a, tw, score);
         } else if (r == 2) {
-          if ((rc = allow_smem(k_big<512, false, S, true>, sm16))) return rc;
-          k_big<512, false, S, true><<<grid, 512, sm16, s>>>(a, tw, score);
+          if (pf) {
+            if ((rc = allow_smem(k_big<512, false, S, true, pf_ok>, sm16))) return rc;
+            k_big<512, false, S, true, pf_ok><<<grid, 512, sm16, s>>>(a, tw, score);
+          } else {
+            if ((rc = allow_smem(k_big<512, false, S, true>, sm16))) return rc;
+            k_big<512, false, S, true><<<grid, 512, sm16, s>>>(a, tw, score);
+          }
         } else {
-          if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
-          k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
+          if (pf) {
+            if ((rc = allow_smem(k_big<1024, false, S, true, pf_ok>, sm16))) return rc;
+            k_big<1024, false, S, true, pf_ok><<<grid, 1024, sm16, s>>>(a, tw, score);
+          } else {
+            if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
+            k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
+          }
         }
       } else if (r < 2) {
-        k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
+        if (pf) k_big<256, W, S, false, pf_ok><<<grid, 256, smr, s>>>(a, tw, score);
+        else k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
       } else if (r == 2) {
         if ((rc = allow_smem(k_big<512, W, S>, smr))) return rc;
         k_big<512, W, S><<<grid, 512, smr, s>>>(a, tw, score);
@@ -555,8 +571,13 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
         k_big<1024, W, S><<<grid, 1024, smr, s>>>(a, tw, score);
       } else if constexpr (!W) {  // the 16-bit range: unweighted graphs only
         const size_t sm16 = (size_t)kBig16Slots * 6;
-        if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
-        k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
+        if (pf) {
+          if ((rc = allow_smem(k_big<1024, false, S, true, pf_ok>, sm16))) return rc;
+          k_big<1024, false, S, true, pf_ok><<<grid, 1024, sm16, s>>>(a, tw, score);
+        } else {
+          if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
+          k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
+        }
       } else {
         set_error("weighted graph with big-tier degrees above %d", kBigMaxWeighted);
         return GLP_EINVAL;
@@ -572,11 +593,21 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     if ((rc = mark_on(s, 3, 0))) return rc;
     const unsigned grid = (unsigned)std::min<int64_t>(cdiv(p.mid.n, kMidNT / 32), kMaxGrid);
     bool c16w = false;  // weighted classic with small weight sums: 16-bit counts
+    const TierWork mw = work(p.mid, 3, &p.fmid);
     if constexpr (W && S::kPacked) {
       c16w = p.mid_c16;
-      if (c16w) k_mid<kMidCap, kMidNT, W, S, true><<<grid, kMidNT, 0, s>>>(a, work(p.mid, 3, &p.fmid), score);
+      if (c16w) k_mid<kMidCap, kMidNT, W, S, true><<<grid, kMidNT, 0, s>>>(a, mw, score);
     }
-    if (!c16w) k_mid<kMidCap, kMidNT, W, S><<<grid, kMidNT, 0, s>>>(a, work(p.mid, 3, &p.fmid), score);
+    if (!c16w) {
+      // the next vertex's first batch in flight while counting: unweighted
+      // classic only (the other instantiations would spill at their register caps)
+      if constexpr (S::kPacked && !W) {
+        if (L.mid_prefetch) k_mid<kMidCap, kMidNT, W, S, true, true><<<grid, kMidNT, 0, s>>>(a, mw, score);
+        else k_mid<kMidCap, kMidNT, W, S><<<grid, kMidNT, 0, s>>>(a, mw, score);
+      } else {
+        k_mid<kMidCap, kMidNT, W, S><<<grid, kMidNT, 0, s>>>(a, mw, score);
+      }
+    }
     if ((rc = mark_on(s, 3, 1))) return rc;
     ++*launches;
   }
@@ -637,6 +668,7 @@ struct RunCtx {
   bool serial = false;                  // glp_params.serial_step: one stream per step
   uint32_t majority_pm = 500, frontier_pm = 50;  // glp_params step-mode thresholds
   bool l2_window = false;               // glp_params.l2_window
+  bool mid_prefetch = true;             // glp_params.mid_prefetch
   bool cycle = false;                   // stop a classic run once it ends in a two-step cycle
   int32_t cycle_from = -1;              // first iteration not run (the labels repeat from there)
 
@@ -679,6 +711,7 @@ struct RunCtx {
     L.serial = serial;
     L.majority_pm = majority_pm;
     L.frontier_pm = frontier_pm;
+    L.mid_prefetch = mid_prefetch;
     return L;
   }
   cudaEvent_t* current() { return timing && used ? evs[used - 1].data() : nullptr; }
@@ -1856,6 +1889,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   if (p.frontier_permille > 0) c.frontier_pm = (uint32_t)std::min(p.frontier_permille, 1000);
   c.l2_window = p.l2_window != 0;
   c.cycle = !p.async && p.cycle_stop == 0;
+  c.mid_prefetch = p.mid_prefetch == 0;
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;

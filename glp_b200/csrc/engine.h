@@ -111,6 +111,7 @@ struct StepLaunch {
   int32_t backend = GLP_BACKEND_EXACT;  // GLP_BACKEND_CM / _FA: summary screen on the big tier
   bool serial = false;  // every kernel on `stream` (per-tier timing without overlap)
   uint32_t majority_pm = 500, frontier_pm = 50;  // step-mode thresholds (changes per 1000 vertices)
+  bool mid_prefetch = true;  // k_mid loads the next vertex's first batch while counting
 };
 
 template <bool W, class S>

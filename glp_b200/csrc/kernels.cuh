@@ -466,8 +466,13 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
 // C16: 16-bit counts (unweighted: a count never exceeds the degree;
 // weighted: the caller knows every mid vertex's weights sum below 2^16), so
 // that the tables and 32 registers a thread fit eight blocks per SM.
-template <int CAP, int NT, bool W, class S, bool C16 = (S::kPacked && !W)>
-__global__ void __launch_bounds__(NT, S::kPacked ? (C16 ? 2048 : 1536) / NT : 1024 / NT)
+// PF: the first batch of the warp's next vertex (its columns, then its
+// neighbour labels) is loaded before the current vertex is counted, so the
+// label gathers are in flight while the table work runs; it costs registers
+// (at most 40 a thread: six blocks per SM).
+template <int CAP, int NT, bool W, class S, bool C16 = (S::kPacked && !W), bool PF = false>
+__global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
+                                         : (S::kPacked ? (C16 ? 2048 : 1536) / NT : 1024 / NT))
     k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
   const bool scan = S::kScan && scan_scores(a);
@@ -478,11 +483,55 @@ __global__ void __launch_bounds__(NT, S::kPacked ? (C16 ? 2048 : 1536) / NT : 10
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
+  const int32_t stride = gridDim.x * NW;
   uint32_t* kk = skeys[warp];
   uint32_t* vv = svals[warp];
-  for (int32_t i = blockIdx.x * NW + warp; i < nwork; i += gridDim.x * NW) {
-    const int32_t v = tw.at(mode, i);
-    const int32_t b = a.off[v], e = a.off[v + 1];
+  // batch loader: columns (and weights) of entries j0 + 32q + lane below e,
+  // then their labels (-1 past the row)
+  auto load_batch = [&](int32_t j0, int32_t e, int32_t (&lab)[4], uint32_t (&wt)[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int32_t j = j0 + 32 * q + lane;
+      lab[q] = j < e ? ld_stream(a.cols + j) : -1;
+      wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
+  };
+  int32_t pv = 0, pb = 0, pe = 0;  // PF: the next vertex and its first batch
+  int32_t plab[4];
+  uint32_t pwt[4];
+  auto prefetch = [&](int32_t idx) {
+    pb = pe = 0;
+    if (idx < nwork) {
+      pv = tw.at(mode, idx);
+      pb = a.off[pv];
+      pe = a.off[pv + 1];
+    }
+    load_batch(pb, pe, plab, pwt);
+  };
+  int32_t i = blockIdx.x * NW + warp;
+  if (PF) prefetch(i);
+  for (; i < nwork; i += stride) {
+    int32_t v, b, e;
+    int32_t lab0[4];
+    uint32_t wt0[4];
+    if (PF) {
+      v = pv;
+      b = pb;
+      e = pe;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        lab0[q] = plab[q];
+        wt0[q] = pwt[q];
+      }
+      prefetch(i + stride);  // in flight while this vertex is counted
+    } else {
+      v = tw.at(mode, i);
+      b = a.off[v];
+      e = a.off[v + 1];
+    }
     const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));  // degree > 32: cap >= 128
     zero_words16(kk, cap, lane, 32);
     zero_words16(vv, C16 ? cap / 2 : cap, lane, 32);
@@ -495,15 +544,15 @@ __global__ void __launch_bounds__(NT, S::kPacked ? (C16 ? 2048 : 1536) / NT : 10
     for (int32_t j0 = b; j0 < e; j0 += 128) {
       int32_t lab[4];
       uint32_t wt[4];
+      if (PF && j0 == b) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int32_t j = j0 + 32 * q + lane;
-        lab[q] = j < e ? ld_stream(a.cols + j) : -1;
-        wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
+        for (int q = 0; q < 4; ++q) {
+          lab[q] = lab0[q];
+          wt[q] = wt0[q];
+        }
+      } else {
+        load_batch(j0, e, lab, wt);
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         if (j0 + 32 * q < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
@@ -545,9 +594,16 @@ __device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32
 // Unweighted classic blocks are held to 32 registers (2048 threads per SM),
 // weighted classic blocks of up to 512 threads to 42 (1536), which they fit
 // without spilling; the other instantiations to 64 (1024 threads per SM).
+// PF: each warp loads its first batch of the block's next vertex (columns,
+// then neighbour labels) before the current vertex is counted, so the label
+// gathers are in flight while the table work runs (unweighted classic; 42
+// registers a thread instead of 32).
 constexpr uint32_t kBig16Slots = 32768;
-template <int NT, bool W, class S, bool C16 = false>
-__global__ void __launch_bounds__(NT, (S::kPacked && !W) ? 2048 / NT : (S::kPacked && NT <= 512) ? 1536 / NT : 1024 / NT) k_big(StepArgs a, TierWork tw, S score) {
+template <int NT, bool W, class S, bool C16 = false, bool PF = false>
+__global__ void __launch_bounds__(NT, PF ? 1536 / NT
+                                         : (S::kPacked && !W) ? 2048 / NT
+                                         : (S::kPacked && NT <= 512) ? 1536 / NT : 1024 / NT)
+    k_big(StepArgs a, TierWork tw, S score) {
   static_assert(!(C16 && W), "16-bit counts hold unweighted counts only");
   const bool scan = S::kScan && scan_scores(a);
   extern __shared__ __align__(16) uint32_t smem[];
@@ -562,9 +618,50 @@ __global__ void __launch_bounds__(NT, (S::kPacked && !W) ? 2048 / NT : (S::kPack
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
+  // first counting round of a vertex: entries j0 + q*NT + lane, j0 = b + 32*warp
+  auto load_round = [&](int32_t j0, int32_t e, int32_t (&lab)[4], uint32_t (&wt)[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int32_t j = j0 + q * NT + lane;
+      lab[q] = j < e ? ld_stream(a.cols + j) : -1;
+      wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
+  };
+  int32_t pv = 0, pb = 0, pe = 0;  // PF: the block's next vertex and this warp's first round of it
+  int32_t plab[4];
+  uint32_t pwt[4];
+  auto prefetch = [&](int32_t idx) {
+    pb = pe = 0;
+    if (idx < nwork) {
+      pv = tw.at(mode, idx);
+      pb = a.off[pv];
+      pe = a.off[pv + 1];
+    }
+    load_round(pb + warp * 32, pe, plab, pwt);
+  };
+  if (PF) prefetch(blockIdx.x);
   for (int32_t i = blockIdx.x; i < nwork; i += gridDim.x) {
-    const int32_t v = tw.at(mode, i);
-    const int32_t b = a.off[v], e = a.off[v + 1];
+    int32_t v, b, e;
+    int32_t lab0[4];
+    uint32_t wt0[4];
+    if (PF) {
+      v = pv;
+      b = pb;
+      e = pe;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        lab0[q] = plab[q];
+        wt0[q] = pwt[q];
+      }
+      prefetch(i + gridDim.x);  // in flight while this vertex is counted
+    } else {
+      v = tw.at(mode, i);
+      b = a.off[v];
+      e = a.off[v + 1];
+    }
     if (S::kMajority && mode == kModeFrontier) {
       // a frontier vertex of this tier has many neighbours and usually keeps
       // its label: a strict majority of its own label decides it without a
@@ -622,15 +719,15 @@ __global__ void __launch_bounds__(NT, (S::kPacked && !W) ? 2048 / NT : (S::kPack
     for (int32_t j0 = b + warp * 32; j0 < e; j0 += 4 * NT) {
       int32_t lab[4];
       uint32_t wt[4];
+      if (PF && j0 == b + warp * 32) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int32_t j = j0 + q * NT + lane;
-        lab[q] = j < e ? ld_stream(a.cols + j) : -1;
-        wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
+        for (int q = 0; q < 4; ++q) {
+          lab[q] = lab0[q];
+          wt[q] = wt0[q];
+        }
+      } else {
+        load_round(j0, e, lab, wt);
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         if (j0 + q * NT < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);

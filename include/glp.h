@@ -119,6 +119,10 @@ typedef struct glp_params {
                                      stream instead of three forked streams, so that
                                      the per-tier event times of glp_outputs are each
                                      tier's own duration (profiling; slower) */
+  int32_t mid_prefetch;           /* mid tier of unweighted classic steps: 0 (default) loads the next
+                                     vertex's first 128 neighbour labels while the current vertex is
+                                     counted; -1 loads them in turn */
+  int32_t reserved[7];            /* zero */
 } glp_params;
 
 /* Per-iteration observer (parity checks).  labels is a HOST copy of the

@@ -427,3 +427,17 @@ def test_two_step_cycle_stop_is_exact(scale):
     np.testing.assert_array_equal(a.labels, otr[-1])
     np.testing.assert_array_equal(a.changed, b.changed)
     assert a.launches < b.launches
+
+
+@pytest.mark.parametrize("pf", [0, -1])
+@pytest.mark.parametrize("case", ["rmat14", "ladder", "planted20k", "star_ring_3000"])
+def test_prefetching_tier_kernels_keep_labels(case, pf):
+    """The mid and big tiers with (default) and without the next-vertex
+    prefetch give the oracle's labels after every iteration, in full-count
+    steps and in majority / frontier steps."""
+    off, cols = CASES[case]
+    niter = 8
+    res, tr = _run_trace(off, cols, _lib.METHOD_CLASSIC, niter, mid_prefetch=pf, cycle_stop=-1)
+    _, otr = O.classic_run(off, cols, niter, trace=True)
+    for it in range(niter):
+        np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
