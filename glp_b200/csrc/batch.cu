@@ -1163,3 +1163,21 @@ int glp_batch_tune(glp_batch* b, int32_t probe_iters, glp_params* best, float* t
 }
 
 }  // extern "C"
+
+namespace glp {
+// Recreates a batch's stream at `priority` once its work has finished (the
+// server's batched rounds run at the device's highest priority).  Not part of
+// the C ABI.
+int batch_set_stream_priority(glp_batch* b, int priority) {
+  if (!b) {
+    set_error("batch is NULL");
+    return GLP_EINVAL;
+  }
+  GLP_BCUDA(cudaStreamSynchronize(b->stream));
+  cudaStream_t fresh = nullptr;
+  GLP_BCUDA(cudaStreamCreateWithPriority(&fresh, cudaStreamNonBlocking, priority));
+  cudaStreamDestroy(b->stream);
+  b->stream = fresh;
+  return GLP_OK;
+}
+}  // namespace glp

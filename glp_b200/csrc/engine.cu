@@ -406,8 +406,8 @@ static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 // One launch over a device-built list of big-tier vertices (majority
 // failures, frontier members, screen fallbacks): 512-thread blocks with a
 // table for the tier's largest degree, with 16-bit counts on unweighted
-// graphs when the tier reaches past kBigMaxWeighted or the score is classic
-// (smaller tables, more blocks per SM).
+// graphs when the tier reaches past kBigMaxWeighted or the score packs
+// (classic, 32-bit layered): smaller tables, more blocks per SM.
 template <bool W, class S>
 static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWork& tw, const S& score,
                            cudaStream_t s, int64_t* launches) {
@@ -525,8 +525,8 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     static_assert(kBigParts == 5 && kBigPartThreads[0] == 256 && kBigPartThreads[1] == 256 &&
                       kBigPartThreads[2] == 512 && kBigPartThreads[3] == 1024 && kBigPartThreads[4] == 1024,
                   "the launches below follow kBigPartThreads");
-    // unweighted classic counts fit 16 bits: from the second range on, the
-    // smaller 16-bit tables (and 32 registers a thread) fit twice the blocks
+    // unweighted counts fit 16 bits: from the second range on, the smaller
+    // 16-bit tables (and S::kSMThreads threads per SM) fit more blocks
     constexpr bool k16 = !W && S::kPacked;
     for (int r = 0; r < kBigParts; ++r) {
       const Verts& vs = p.big_part[r];
@@ -534,35 +534,19 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       const TierWork tw{vs, none, none, 1};
       const size_t smr = 4ull * kBigPartMax[r] * sizeof(uint32_t);
       const unsigned grid = (unsigned)std::min<int64_t>(vs.n, kMaxGrid);
-      // unweighted classic: each warp's first round of the next vertex is in
-      // flight while the current one is counted (L.mid_prefetch)
-      constexpr bool pf_ok = !W && S::kPacked;
-      const bool pf = pf_ok && L.mid_prefetch;
       if (k16 && r > 0 && r < kBigParts - 1) {
         const size_t sm16 = 12ull * kBigPartMax[r];  // 2*max slots of 4 + 2 bytes
         if (r == 1) {
-          if (pf) k_big<256, false, S, true, pf_ok><<<grid, 256, sm16, s>>>(a, tw, score);
-          else k_big<256, false, S, true><<<grid, 256, sm16, s>>>(a, tw, score);
+          k_big<256, false, S, true><<<grid, 256, sm16, s>>>(a, tw, score);
         } else if (r == 2) {
-          if (pf) {
-            if ((rc = allow_smem(k_big<512, false, S, true, pf_ok>, sm16))) return rc;
-            k_big<512, false, S, true, pf_ok><<<grid, 512, sm16, s>>>(a, tw, score);
-          } else {
-            if ((rc = allow_smem(k_big<512, false, S, true>, sm16))) return rc;
-            k_big<512, false, S, true><<<grid, 512, sm16, s>>>(a, tw, score);
-          }
+          if ((rc = allow_smem(k_big<512, false, S, true>, sm16))) return rc;
+          k_big<512, false, S, true><<<grid, 512, sm16, s>>>(a, tw, score);
         } else {
-          if (pf) {
-            if ((rc = allow_smem(k_big<1024, false, S, true, pf_ok>, sm16))) return rc;
-            k_big<1024, false, S, true, pf_ok><<<grid, 1024, sm16, s>>>(a, tw, score);
-          } else {
-            if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
-            k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
-          }
+          if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
+          k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
         }
       } else if (r < 2) {
-        if (pf) k_big<256, W, S, false, pf_ok><<<grid, 256, smr, s>>>(a, tw, score);
-        else k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
+        k_big<256, W, S><<<grid, 256, smr, s>>>(a, tw, score);
       } else if (r == 2) {
         if ((rc = allow_smem(k_big<512, W, S>, smr))) return rc;
         k_big<512, W, S><<<grid, 512, smr, s>>>(a, tw, score);
@@ -571,13 +555,8 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
         k_big<1024, W, S><<<grid, 1024, smr, s>>>(a, tw, score);
       } else if constexpr (!W) {  // the 16-bit range: unweighted graphs only
         const size_t sm16 = (size_t)kBig16Slots * 6;
-        if (pf) {
-          if ((rc = allow_smem(k_big<1024, false, S, true, pf_ok>, sm16))) return rc;
-          k_big<1024, false, S, true, pf_ok><<<grid, 1024, sm16, s>>>(a, tw, score);
-        } else {
-          if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
-          k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
-        }
+        if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
+        k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
       } else {
         set_error("weighted graph with big-tier degrees above %d", kBigMaxWeighted);
         return GLP_EINVAL;
@@ -601,7 +580,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     if (!c16w) {
       // the next vertex's first batch in flight while counting: unweighted
       // classic only (the other instantiations would spill at their register caps)
-      if constexpr (S::kPacked && !W) {
+      if constexpr (S::kMajority && !W) {
         if (L.mid_prefetch) k_mid<kMidCap, kMidNT, W, S, true, true><<<grid, kMidNT, 0, s>>>(a, mw, score);
         else k_mid<kMidCap, kMidNT, W, S><<<grid, kMidNT, 0, s>>>(a, mw, score);
       } else {
@@ -842,34 +821,45 @@ static int ensure_sorted(glp_graph* g) {
 // ascending: unweighted, the row's last column (k_first_step); weighted, the
 // row's largest (weight, label), per tier: a thread per vertex up to degree
 // 32, a warp per mid vertex, a block per big vertex and hub.
-template <bool W>
-static int launch_first_step(const DevicePlan& p, const StepArgs& a, cudaStream_t s, int64_t* launches) {
+// Per tier, the neighbour of largest key (a thread per vertex up to degree
+// 32, a warp per mid vertex, a block per big vertex and hub).
+template <class K>
+static int launch_first_keyed(const DevicePlan& p, const StepArgs& a, const K& key, cudaStream_t s,
+                              int64_t* launches) {
   const unsigned kMaxGrid = device_sms() * 32;
-  if constexpr (!W) {
-    k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), kMaxGrid), 256, 0, s>>>(a);
+  for (const Verts* vs : {&p.tiny, &p.g16, &p.g32})
+    if (vs->n) {
+      k_first_step_w<1, K><<<(unsigned)std::min<int64_t>(cdiv(vs->n, 256), kMaxGrid), 256, 0, s>>>(a, *vs, key);
+      ++*launches;
+    }
+  if (p.mid.n) {
+    k_first_step_w<32, K><<<(unsigned)std::min<int64_t>(cdiv((int64_t)p.mid.n * 32, 256), kMaxGrid), 256, 0, s>>>(
+        a, p.mid, key);
     ++*launches;
-  } else {
-    for (const Verts* vs : {&p.tiny, &p.g16, &p.g32})
-      if (vs->n) {
-        k_first_step_w<1><<<(unsigned)std::min<int64_t>(cdiv(vs->n, 256), kMaxGrid), 256, 0, s>>>(a, *vs);
-        ++*launches;
-      }
-    if (p.mid.n) {
-      k_first_step_w<32><<<(unsigned)std::min<int64_t>(cdiv((int64_t)p.mid.n * 32, 256), kMaxGrid), 256, 0, s>>>(
-          a, p.mid);
-      ++*launches;
-    }
-    if (p.big.n) {
-      k_first_step_w_block<256><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), 256, 0, s>>>(a, p.big);
-      ++*launches;
-    }
-    if (p.n_hubs) {
-      k_first_step_w_block<1024><<<(unsigned)p.n_hubs, 1024, 0, s>>>(a, Verts{p.hub.hub_v, 0, p.n_hubs});
-      ++*launches;
-    }
+  }
+  if (p.big.n) {
+    k_first_step_w_block<256, K><<<(unsigned)std::min<int64_t>(p.big.n, kMaxGrid), 256, 0, s>>>(a, p.big, key);
+    ++*launches;
+  }
+  if (p.n_hubs) {
+    k_first_step_w_block<1024, K><<<(unsigned)p.n_hubs, 1024, 0, s>>>(a, Verts{p.hub.hub_v, 0, p.n_hubs}, key);
+    ++*launches;
   }
   GLP_CUDA(cudaGetLastError());
   return GLP_OK;
+}
+
+template <bool W>
+static int launch_first_step(const DevicePlan& p, const StepArgs& a, cudaStream_t s, int64_t* launches) {
+  if constexpr (!W) {
+    const unsigned kMaxGrid = device_sms() * 32;
+    k_first_step<<<(unsigned)std::min<int64_t>(cdiv(a.n, 256), kMaxGrid), 256, 0, s>>>(a);
+    ++*launches;
+    GLP_CUDA(cudaGetLastError());
+    return GLP_OK;
+  } else {
+    return launch_first_keyed(p, a, FirstKeyW{}, s, launches);
+  }
 }
 
 // The first step as its own timed step.
@@ -1037,6 +1027,9 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
   int32_t step = 0;
   int32_t* final_lab = g->d_lab[0];
   for (int32_t layer = 0; layer < p.nlayers; ++layer) {
+    // 32-bit scores when every score of the layer fits them: a count is at
+    // most a row's weight sum, a volume at most n
+    const bool narrow = (int64_t)p.dstar[layer] * g->max_wsum + g->n < 2147483648LL;
     if ((rc = init_labels(c))) return rc;
     for (int32_t it = 0; it < niter; ++it, ++step) {
       if (step > 0) {
@@ -1054,7 +1047,18 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       L.prev_changed = it > 0 ? g->d_changed + step - 1 : nullptr;
       L.allow_majority = 0;
       L.allow_frontier = 0;
-      if ((rc = launch_step<W>(L, a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches))) return rc;
+      if (it == 0 && narrow && g->rows_sorted == 1) {
+        // labels = ids and no repeated neighbour: every label occurs once, so
+        // the step is a streaming maximum of dstar*w - vol_r[neighbour]
+        if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[16], c.s));
+        rc = launch_first_keyed(g->plan, a, FirstKeyLayered<W>{vol_r, p.dstar[layer]}, c.s, &c.launches);
+        if (!rc && L.ev) GLP_CUDA(cudaEventRecord(L.ev[17], c.s));
+      } else if (narrow) {
+        rc = launch_step<W>(L, a, ScoreLayered32{vol_r, p.dstar[layer]}, &c.launches);
+      } else {
+        rc = launch_step<W>(L, a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches);
+      }
+      if (rc) return rc;
       if ((rc = c.aux_mark(0))) return rc;
       k_histogram<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(lout, g->n, vol_w);
       ++c.launches;
@@ -1155,9 +1159,10 @@ __global__ void k_validate_offsets(const int32_t* __restrict__ off, int32_t n, i
 // Columns in [0, n) (bad 1), weights >= 0 (bad 2), per-vertex weight sums
 // below 2^31 (bad 4).  Runs only on valid offsets.
 // mid_wsum: the largest weight sum of a vertex of degree <= kMidCap / 2 (a
-// bound on any of its label counts).
+// bound on any of its label counts); max_wsum: the largest of any vertex.
 __global__ void k_validate(const int32_t* __restrict__ off, const int32_t* __restrict__ cols,
-                           const int32_t* __restrict__ w, int64_t m, int32_t n, uint32_t* bad, uint32_t* mid_wsum) {
+                           const int32_t* __restrict__ w, int64_t m, int32_t n, uint32_t* bad, uint32_t* mid_wsum,
+                           uint32_t* max_wsum) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
     const int32_t c = cols[j];
     if (c < 0 || c >= n) atomicOr(bad, 1u);
@@ -1165,19 +1170,22 @@ __global__ void k_validate(const int32_t* __restrict__ off, const int32_t* __res
   }
   // the engine sums a vertex's weights in 32 bits
   if (w) {
-    uint32_t mid_max = 0;
+    uint32_t mid_max = 0, all_max = 0;
     const int32_t nv = (n + 31) & ~31;  // whole warps for the reduction
     for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
       if (v < n) {
         int64_t sum = 0;
         for (int32_t j = off[v]; j < off[v + 1]; ++j) sum += w[j];
         if (sum >= 2147483648LL) atomicOr(bad, 4u);
-        if (off[v + 1] - off[v] <= kMidCap / 2 && sum > 0)
-          mid_max = max(mid_max, sum < 0xffffffffLL ? (uint32_t)sum : 0xffffffffu);
+        const uint32_t s32 = sum < 0xffffffffLL ? (uint32_t)sum : 0xffffffffu;
+        if (off[v + 1] - off[v] <= kMidCap / 2 && sum > 0) mid_max = max(mid_max, s32);
+        all_max = max(all_max, s32);
       }
     }
     mid_max = __reduce_max_sync(kFull, mid_max);
+    all_max = __reduce_max_sync(kFull, all_max);
     if ((threadIdx.x & 31) == 0 && mid_max) atomicMax(mid_wsum, mid_max);
+    if ((threadIdx.x & 31) == 0 && all_max) atomicMax(max_wsum, all_max);
   }
 }
 
@@ -1187,6 +1195,7 @@ int validate_csr_device(glp_graph* g) {
     int32_t maxdeg;
     uint32_t unsorted;
     uint32_t mid_wsum;
+    uint32_t max_wsum;
   };
   Flags* d_f = nullptr;
   GLP_CUDA(dev_alloc(&d_f, sizeof(Flags)));
@@ -1195,7 +1204,7 @@ int validate_csr_device(glp_graph* g) {
   Flags f{};
   cudaError_t e = cudaMemcpy(&f, d_f, sizeof f, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && !f.bad && g->m) {
-    k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, &d_f->bad, &d_f->mid_wsum);
+    k_validate<<<1184, 256>>>(g->d_off, g->d_cols, g->d_w, g->m, g->n, &d_f->bad, &d_f->mid_wsum, &d_f->max_wsum);
     e = cudaMemcpy(&f, d_f, sizeof f, cudaMemcpyDeviceToHost);
   }
   dev_free(d_f);
@@ -1223,6 +1232,7 @@ int validate_csr_device(glp_graph* g) {
   g->max_degree = f.maxdeg;
   g->deg_sorted = f.unsorted ? 0 : 1;
   g->mid_wsum = f.mid_wsum;
+  g->max_wsum = g->d_w ? f.max_wsum : (uint32_t)f.maxdeg;
   return GLP_OK;
 }
 
@@ -1893,7 +1903,9 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;
-  if ((method == GLP_METHOD_CLASSIC || method == GLP_METHOD_SLPA) && (rc = ensure_sorted(g))) return rc;
+  if ((method == GLP_METHOD_CLASSIC || method == GLP_METHOD_SLPA || method == GLP_METHOD_LAYERED) &&
+      (rc = ensure_sorted(g)))
+    return rc;
   if (method == GLP_METHOD_CLASSIC && (rc = ensure_symmetric(g))) return rc;
   switch (method) {
     case GLP_METHOD_CLASSIC:
@@ -2003,7 +2015,7 @@ int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int
     return GLP_OK;
   }
   k_validate_offsets<<<1184, 256, 0, st>>>(d_offsets, n, m, &sc->bad, &sc->maxdeg, &sc->unsorted);
-  if (m) k_validate<<<1184, 256, 0, st>>>(d_offsets, d_cols, nullptr, m, n, &sc->bad, nullptr);
+  if (m) k_validate<<<1184, 256, 0, st>>>(d_offsets, d_cols, nullptr, m, n, &sc->bad, nullptr, nullptr);
   GLP_CUDA(cudaGetLastError());
   uint32_t flags[2] = {0, 0};  // bad, maxdeg
   GLP_CUDA(cudaMemcpyAsync(flags, &sc->bad, sizeof flags, cudaMemcpyDeviceToHost, st));
@@ -2048,3 +2060,27 @@ int glp_run_classic_noalloc(const int32_t* d_offsets, const int32_t* d_cols, int
 }
 
 }  // extern "C"
+
+namespace glp {
+// Recreates a handle's three streams at `priority` (the order of
+// cudaDeviceGetStreamPriorityRange: lower is more urgent) once its work has
+// finished.  Not part of the C ABI: the server runs short requests at the
+// device's highest priority, so that the block scheduler dispatches their
+// blocks ahead of the queued blocks of a long solve sharing the GPU.
+int graph_set_stream_priority(glp_graph* g, int priority) {
+  if (!g) {
+    set_error("graph is NULL");
+    return GLP_EINVAL;
+  }
+  int rc = quiesce(g);
+  if (rc) return rc;
+  g->last_stream = nullptr;
+  for (cudaStream_t* st : {&g->stream, &g->aux[0], &g->aux[1]}) {
+    cudaStream_t fresh = nullptr;
+    GLP_CUDA(cudaStreamCreateWithPriority(&fresh, cudaStreamNonBlocking, priority));
+    if (*st) cudaStreamDestroy(*st);
+    *st = fresh;
+  }
+  return GLP_OK;
+}
+}  // namespace glp

@@ -183,11 +183,18 @@ struct ScoreClassic {
   // reduce with one 64-bit shared atomicMax
   static constexpr bool kPacked = true;
   static constexpr bool kScan = false;  // no lookup: running maximum at every insert
+  // threads per SM the unweighted mid / big kernels are compiled for (32
+  // registers a thread); their 16-bit count tables fit as many
+  static constexpr int kSMThreads = 2048;
   __device__ __forceinline__ int64_t operator()(int32_t, uint32_t k) const { return (int64_t)k; }
   __device__ __forceinline__ int32_t vol_of(int32_t) const { return 0; }
   __device__ __forceinline__ int64_t from_vol(uint32_t k, int32_t) const { return (int64_t)k; }
   // the largest score a label of count <= k can have
   __device__ __forceinline__ int64_t bound(uint32_t k) const { return (int64_t)k; }
+  // the packed form: counts are non-negative, so (count << 32 | label) is monotone
+  static __device__ __forceinline__ unsigned long long pack(const Best& b) {
+    return ((unsigned long long)b.s << 32) | (uint32_t)b.l;
+  }
 };
 
 // score(l, k) for layered LP: dstar*k - vol_r[l] (kernel.cuh:2575-2600).
@@ -198,6 +205,7 @@ struct ScoreLayered {
   // the volume is a global lookup per label: prefetched per insert, or (step
   // mode word 1) looked up once per distinct label by a scan of the table
   static constexpr bool kScan = true;
+  static constexpr int kSMThreads = 1024;  // 64 registers a thread
   const int32_t* vol;
   int64_t dstar;
   __device__ __forceinline__ int64_t operator()(int32_t l, uint32_t k) const {
@@ -208,6 +216,33 @@ struct ScoreLayered {
   __device__ __forceinline__ int64_t from_vol(uint32_t k, int32_t v) const { return dstar * (int64_t)k - (int64_t)v; }
   // the largest score a label of count <= k can have (volumes are >= 0)
   __device__ __forceinline__ int64_t bound(uint32_t k) const { return dstar * (int64_t)k; }
+  static __device__ __forceinline__ unsigned long long pack(const Best&) { return 0ull; }  // not packed
+};
+
+// The same layered score in 32-bit arithmetic, for graphs where every score
+// lies in [-2^31, 2^31): the host checks |dstar| * (largest weight sum of a
+// row) + n < 2^31 (counts never exceed a row's weight sum, volumes never
+// exceed n).  Scores then pack with their label into one 64-bit word
+// ((score + 2^31) << 32 | label, monotone in (score, label)), so the big tier
+// reduces with one shared atomicMax and the unweighted tables take 16-bit
+// counts, as in classic LP: fewer registers and smaller tables, more blocks
+// per SM.
+struct ScoreLayered32 {
+  static constexpr bool kMajority = false;
+  static constexpr bool kPacked = true;
+  static constexpr bool kScan = true;
+  static constexpr int kSMThreads = 1536;  // 40 registers a thread: 32 would spill
+  const int32_t* vol;
+  int32_t dstar;
+  __device__ __forceinline__ int64_t operator()(int32_t l, uint32_t k) const {
+    return (int64_t)(dstar * (int32_t)k - __ldg(vol + l));
+  }
+  __device__ __forceinline__ int32_t vol_of(int32_t l) const { return __ldg(vol + l); }
+  __device__ __forceinline__ int64_t from_vol(uint32_t k, int32_t v) const { return (int64_t)(dstar * (int32_t)k - v); }
+  __device__ __forceinline__ int64_t bound(uint32_t k) const { return (int64_t)(dstar * (int32_t)k); }
+  static __device__ __forceinline__ unsigned long long pack(const Best& b) {
+    return ((unsigned long long)((uint32_t)(int32_t)b.s ^ 0x80000000u) << 32) | (uint32_t)b.l;
+  }
 };
 
 template <bool W>
@@ -376,11 +411,12 @@ __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, 
 
 // The best (score, label) over the occupied slots of a finished table, slots
 // t, t+stride, ... of it (scores with kScan).
-// Eight slots a round, their volume loads in flight together.
+// Eight slots a round (four in kernels held to 40 registers), their volume
+// loads in flight together.
 template <bool C16 = false, class S>
 __device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t* vals, uint32_t cap, uint32_t t,
                                            uint32_t stride, const S& score, Best& best) {
-  constexpr int U = 8;
+  constexpr int U = S::kSMThreads > 1024 ? 4 : 8;
   for (uint32_t s0 = t; s0 < cap; s0 += U * stride) {
     uint32_t key[U], val[U];
     int32_t vl[U];
@@ -472,7 +508,7 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
 // (at most 40 a thread: six blocks per SM).
 template <int CAP, int NT, bool W, class S, bool C16 = (S::kPacked && !W), bool PF = false>
 __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
-                                         : (S::kPacked ? (C16 ? 2048 : 1536) / NT : 1024 / NT))
+                                         : (C16 ? S::kSMThreads : S::kSMThreads == 2048 ? 1536 : 1024) / NT)
     k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
   const bool scan = S::kScan && scan_scores(a);
@@ -591,18 +627,13 @@ __device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32
 // vertex to the power of two >= 2*degree.  C16 (unweighted counts only):
 // 16-bit counts, and at most kBig16Slots slots (three quarters full at
 // degree 24576), so 24576 labels fit 192 KB of shared memory.
-// Unweighted classic blocks are held to 32 registers (2048 threads per SM),
-// weighted classic blocks of up to 512 threads to 42 (1536), which they fit
-// without spilling; the other instantiations to 64 (1024 threads per SM).
-// PF: each warp loads its first batch of the block's next vertex (columns,
-// then neighbour labels) before the current vertex is counted, so the label
-// gathers are in flight while the table work runs (unweighted classic; 42
-// registers a thread instead of 32).
+// Unweighted blocks are held to S::kSMThreads threads per SM (classic: 32
+// registers, 32-bit layered: 40), weighted classic blocks of up to 512
+// threads to 40 (1536), which they fit without spilling; the other
+// instantiations to 64 (1024 threads per SM).
 constexpr uint32_t kBig16Slots = 32768;
-template <int NT, bool W, class S, bool C16 = false, bool PF = false>
-__global__ void __launch_bounds__(NT, PF ? 1536 / NT
-                                         : (S::kPacked && !W) ? 2048 / NT
-                                         : (S::kPacked && NT <= 512) ? 1536 / NT : 1024 / NT)
+template <int NT, bool W, class S, bool C16 = false>
+__global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 2048 && NT <= 512) ? 1536 : 1024) / NT)
     k_big(StepArgs a, TierWork tw, S score) {
   static_assert(!(C16 && W), "16-bit counts hold unweighted counts only");
   const bool scan = S::kScan && scan_scores(a);
@@ -618,50 +649,9 @@ __global__ void __launch_bounds__(NT, PF ? 1536 / NT
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
-  // first counting round of a vertex: entries j0 + q*NT + lane, j0 = b + 32*warp
-  auto load_round = [&](int32_t j0, int32_t e, int32_t (&lab)[4], uint32_t (&wt)[4]) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int32_t j = j0 + q * NT + lane;
-      lab[q] = j < e ? ld_stream(a.cols + j) : -1;
-      wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
-  };
-  int32_t pv = 0, pb = 0, pe = 0;  // PF: the block's next vertex and this warp's first round of it
-  int32_t plab[4];
-  uint32_t pwt[4];
-  auto prefetch = [&](int32_t idx) {
-    pb = pe = 0;
-    if (idx < nwork) {
-      pv = tw.at(mode, idx);
-      pb = a.off[pv];
-      pe = a.off[pv + 1];
-    }
-    load_round(pb + warp * 32, pe, plab, pwt);
-  };
-  if (PF) prefetch(blockIdx.x);
   for (int32_t i = blockIdx.x; i < nwork; i += gridDim.x) {
-    int32_t v, b, e;
-    int32_t lab0[4];
-    uint32_t wt0[4];
-    if (PF) {
-      v = pv;
-      b = pb;
-      e = pe;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        lab0[q] = plab[q];
-        wt0[q] = pwt[q];
-      }
-      prefetch(i + gridDim.x);  // in flight while this vertex is counted
-    } else {
-      v = tw.at(mode, i);
-      b = a.off[v];
-      e = a.off[v + 1];
-    }
+    const int32_t v = tw.at(mode, i);
+    const int32_t b = a.off[v], e = a.off[v + 1];
     if (S::kMajority && mode == kModeFrontier) {
       // a frontier vertex of this tier has many neighbours and usually keeps
       // its label: a strict majority of its own label decides it without a
@@ -719,15 +709,15 @@ __global__ void __launch_bounds__(NT, PF ? 1536 / NT
     for (int32_t j0 = b + warp * 32; j0 < e; j0 += 4 * NT) {
       int32_t lab[4];
       uint32_t wt[4];
-      if (PF && j0 == b + warp * 32) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          lab[q] = lab0[q];
-          wt[q] = wt0[q];
-        }
-      } else {
-        load_round(j0, e, lab, wt);
+      for (int q = 0; q < 4; ++q) {
+        const int32_t j = j0 + q * NT + lane;
+        lab[q] = j < e ? ld_stream(a.cols + j) : -1;
+        wt[q] = j < e ? (W ? (uint32_t)ld_stream(a.w + j) : 1u) : 0u;
       }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         if (j0 + q * NT < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
@@ -738,10 +728,9 @@ __global__ void __launch_bounds__(NT, PF ? 1536 / NT
       scan_table<C16>(keys, vals, cap, threadIdx.x, NT, score, best);
     }
     if (S::kPacked) {
-      // counts and labels are non-negative: (count << 32 | label) is monotone
+      // S::pack is monotone in (score, label) and never 0 for a candidate
       best = group_max<32>(best);
-      if (lane == 0 && best.l >= 0)
-        atomicMax(&sbest[par], ((unsigned long long)best.s << 32) | (uint32_t)best.l);
+      if (lane == 0 && best.l >= 0) atomicMax(&sbest[par], S::pack(best));
       __syncthreads();
       if (threadIdx.x == 0) best.l = (int32_t)(uint32_t)sbest[par];
       par ^= 1;
@@ -1109,12 +1098,29 @@ __global__ void __launch_bounds__(256) k_first_step(StepArgs a) {
 // The weighted form of the same shortcut: every neighbour label occurs once,
 // so its count is the edge's weight, and the step takes the neighbour label
 // of largest (weight, label).  G lanes per vertex (1 or 32); the rows of the
-// big tier and the hubs go to k_first_step_w_block.
-__device__ __forceinline__ unsigned long long first_key_w(const StepArgs& a, int32_t j) {
-  return ((unsigned long long)(uint32_t)a.w[j] << 32) | (uint32_t)a.lin[a.cols[j]];
-}
-template <int G>
-__global__ void __launch_bounds__(256) k_first_step_w(StepArgs a, Verts vs) {
+// big tier and the hubs go to k_first_step_w_block.  The key of an entry is
+// a 64-bit word monotone in (score, label) and never 0 for a candidate.
+struct FirstKeyW {
+  __device__ __forceinline__ unsigned long long operator()(const StepArgs& a, int32_t j) const {
+    return ((unsigned long long)(uint32_t)a.w[j] << 32) | (uint32_t)a.lin[a.cols[j]];
+  }
+};
+// Layered LP at the start of a layer: every label occurs once, so label l of
+// edge weight k (1 unweighted) scores dstar*k - vol_r[l], in 32 bits (the host
+// checks the range) and packed as ScoreLayered32::pack does.
+template <bool W>
+struct FirstKeyLayered {
+  const int32_t* vol;
+  int32_t dstar;
+  __device__ __forceinline__ unsigned long long operator()(const StepArgs& a, int32_t j) const {
+    const int32_t l = ld_label(a.lin + ld_stream(a.cols + j));
+    const int32_t k = W ? ld_stream(a.w + j) : 1;
+    const int32_t sc = dstar * k - __ldg(vol + l);
+    return ((unsigned long long)((uint32_t)sc ^ 0x80000000u) << 32) | (uint32_t)l;
+  }
+};
+template <int G, class K = FirstKeyW>
+__global__ void __launch_bounds__(256) k_first_step_w(StepArgs a, Verts vs, K key = K{}) {
   const int lane = threadIdx.x & (G - 1);
   for (int64_t t0 = (int64_t)blockIdx.x * blockDim.x; t0 < (int64_t)vs.n * G; t0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = (t0 + threadIdx.x) / G;
@@ -1124,7 +1130,7 @@ __global__ void __launch_bounds__(256) k_first_step_w(StepArgs a, Verts vs) {
     if (i < vs.n) {
       v = vs[i];
       const int32_t b = a.off[v], e = a.off[v + 1];
-      for (int32_t j = b + lane; j < e; j += G) best = max(best, first_key_w(a, j));
+      for (int32_t j = b + lane; j < e; j += G) best = max(best, key(a, j));
     }
 #pragma unroll
     for (int m = G / 2; m >= 1; m >>= 1) best = max(best, __shfl_xor_sync(kFull, best, m));
@@ -1136,8 +1142,8 @@ __global__ void __launch_bounds__(256) k_first_step_w(StepArgs a, Verts vs) {
     record_changes(a, chg, v);
   }
 }
-template <int NT>
-__global__ void __launch_bounds__(NT) k_first_step_w_block(StepArgs a, Verts vs) {
+template <int NT, class K = FirstKeyW>
+__global__ void __launch_bounds__(NT) k_first_step_w_block(StepArgs a, Verts vs, K key = K{}) {
   __shared__ unsigned long long sb;
   for (int32_t i = blockIdx.x; i < vs.n; i += gridDim.x) {
     const int32_t v = vs[i];
@@ -1145,7 +1151,7 @@ __global__ void __launch_bounds__(NT) k_first_step_w_block(StepArgs a, Verts vs)
     if (threadIdx.x == 0) sb = 0ull;
     __syncthreads();
     unsigned long long best = 0ull;
-    for (int32_t j = b + threadIdx.x; j < e; j += NT) best = max(best, first_key_w(a, j));
+    for (int32_t j = b + threadIdx.x; j < e; j += NT) best = max(best, key(a, j));
 #pragma unroll
     for (int m = 16; m >= 1; m >>= 1) best = max(best, __shfl_xor_sync(kFull, best, m));
     if ((threadIdx.x & 31) == 0) atomicMax(&sb, best);

@@ -22,6 +22,13 @@
 //             streams, so their work overlaps with the rounds on the device.
 //             A worker takes the admitted request of the smallest expected
 //             service time, aged by how long it has waited.
+//   short   : one-graph requests expected below short_job_us have a worker
+//             of their own, so that a small layered or SLPA solve does not
+//             wait behind a long one; plain workers take them only when they
+//             have nothing else.
+// The batch thread and the short worker run on streams of the device's
+// highest priority: the block scheduler dispatches their blocks ahead of the
+// queued blocks of a long solve sharing the GPU.
 // A request's host buffers (CSR in, labels out) must stay valid until it is
 // done.  Results are exactly those of glp_run alone: the batched kernel
 // reproduces glp_run(method 1) per graph, and the plain path is glp_run.
@@ -46,6 +53,8 @@
 
 namespace glp {
 void set_error(const char* fmt, ...);
+int graph_set_stream_priority(glp_graph* g, int priority);
+int batch_set_stream_priority(glp_batch* b, int priority);
 int ingest_edges(const int32_t* src, const int32_t* dst, int64_t count, int32_t n, int32_t on_device, uint32_t flags,
                  int32_t** d_off, int32_t** d_cols, int64_t* m, int32_t* d_old, cudaStream_t s);
 }  // namespace glp
@@ -82,6 +91,7 @@ struct Request {
   int32_t* labels = nullptr;
   int32_t max_degree = 0;
   bool batched = false;
+  bool short_job = false;  // one-graph, expected below short_job_us
   int64_t bytes = 0;
   double cost_s = 0;  // expected service time, for shortest-job-first
   volatile int32_t cancel = 0;  // glp_server_cancel: stop (one-graph solve) or discard (batched round)
@@ -104,6 +114,8 @@ struct glp_server {
   std::deque<Request*> pending;     // submitted, not admitted (FIFO)
   std::deque<Request*> batch_q;     // admitted, batched path
   std::deque<Request*> plain_q;     // admitted, plain path
+  std::deque<Request*> short_q;     // admitted, plain path, short jobs
+  int high_priority = 0;            // the device's most urgent stream priority
   std::unordered_map<int64_t, std::unique_ptr<Request>> all;
   std::unordered_map<int64_t, std::unique_ptr<Resident>> graphs;
   std::unordered_set<int64_t> removed_graphs;  // ids whose cached handles must go
@@ -185,7 +197,7 @@ void admit_locked(glp_server* s) {
     s->used_bytes += r->bytes;
     s->in_flight++;
     r->stats.admit_s = s->now();
-    (r->batched ? s->batch_q : s->plain_q).push_back(r);
+    (r->batched ? s->batch_q : r->short_job ? s->short_q : s->plain_q).push_back(r);
     any = true;
   }
   if (any) s->cv_work.notify_all();
@@ -203,6 +215,7 @@ struct OneGraphRunner {
   };
   glp_server* s;
   std::unordered_map<int64_t, Cached> cache;
+  bool urgent = false;  // handles on the device's highest stream priority
 
   void drop(int64_t id) {
     auto it = cache.find(id);
@@ -240,6 +253,10 @@ struct OneGraphRunner {
         g = it->second.g;
       } else {
         rc = glp_graph_create(r->res->d_off, r->res->d_cols, r->res->d_w, r->res->n, r->res->m, 1, &g);
+        if (rc == GLP_OK && urgent && (rc = glp::graph_set_stream_priority(g, s->high_priority)) != GLP_OK) {
+          glp_graph_destroy(g);
+          g = nullptr;
+        }
         if (rc == GLP_OK) {
           const int64_t hb = handle_bytes(*r->res);
           cache.emplace(r->res->id, Cached{g, hb});
@@ -250,6 +267,7 @@ struct OneGraphRunner {
       transient = false;
     } else {
       rc = glp_graph_create(r->offsets, r->cols, r->weights, r->n, r->m, 0, &g);
+      if (rc == GLP_OK && urgent) rc = glp::graph_set_stream_priority(g, s->high_priority);
     }
     if (rc == GLP_OK && r->cancel) {
       glp::set_error("cancelled before it started");
@@ -268,28 +286,32 @@ struct OneGraphRunner {
   }
 };
 
-void plain_worker(glp_server* s) {
+// A plain worker serves plain_q, and short_q when plain_q is empty; the
+// short worker (short_lane) serves short_q only, on urgent streams.
+void plain_worker(glp_server* s, bool short_lane) {
   cudaSetDevice(s->cfg.device);
-  OneGraphRunner one{s, {}};
+  OneGraphRunner one{s, {}, short_lane};
   for (;;) {
     Request* r = nullptr;
     std::vector<int64_t> stale;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_work.wait(lk, [&] { return !s->plain_q.empty() || idle_locked(s); });
+      auto has_work = [&] { return !s->short_q.empty() || (!short_lane && !s->plain_q.empty()); };
+      s->cv_work.wait(lk, [&] { return has_work() || idle_locked(s); });
       stale = one.stale_locked();
-      if (s->plain_q.empty()) {
+      if (!has_work()) {
         lk.unlock();
         one.clear();
         return;
       }
       // shortest expected job first, aged by its wait so none starves
+      std::deque<Request*>& q = (short_lane || s->plain_q.empty()) ? s->short_q : s->plain_q;
       const double now = s->now();
-      auto best = s->plain_q.begin();
-      for (auto it = s->plain_q.begin(); it != s->plain_q.end(); ++it)
+      auto best = q.begin();
+      for (auto it = q.begin(); it != q.end(); ++it)
         if ((*it)->cost_s - (now - (*it)->stats.admit_s) < (*best)->cost_s - (now - (*best)->stats.admit_s)) best = it;
       r = *best;
-      s->plain_q.erase(best);
+      q.erase(best);
       r->stats.start_s = now;
       r->stats.path = 0;
     }
@@ -310,10 +332,15 @@ void batch_worker(glp_server* s) {
   cudaStream_t up = nullptr;  // uploads of host CSRs, finished before packing
   cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
   glp_batch* b = nullptr;     // kept across rounds: repacking reuses its buffers
+  // host CSRs of a round are uploaded into one grow-only staging buffer: no
+  // allocation or free per round (a free waits for every stream of the
+  // device, the one-graph solves of the plain workers included)
+  int32_t* stage = nullptr;
+  size_t stage_cap = 0;  // int32 elements
   // A round of one request runs as a one-graph solve: the persistent kernel
   // is a cooperative launch that needs every SM free, so alone it would wait
   // for whatever else occupies the GPU and gain nothing from batching.
-  OneGraphRunner one{s, {}};
+  OneGraphRunner one{s, {}, true};
   for (;;) {
     std::vector<Request*> round;
     std::vector<int64_t> stale;
@@ -324,6 +351,7 @@ void batch_worker(glp_server* s) {
       if (s->batch_q.empty()) {
         lk.unlock();
         if (up) cudaStreamDestroy(up);
+        cudaFree(stage);
         glp_batch_destroy(b);
         one.clear();
         return;
@@ -357,10 +385,29 @@ void batch_worker(glp_server* s) {
     std::vector<const int32_t*> offs(G), cols(G);
     std::vector<int32_t> ns(G), its(G);
     std::vector<int64_t> ms(G);
-    std::vector<void*> temps;
     int64_t total = 0;
     int rc = GLP_OK;
-    for (size_t i = 0; i < G && rc == GLP_OK; ++i) {
+    // staging layout: per host request, offsets then columns, each segment
+    // starting on a 64-element (256-byte) boundary
+    auto seg = [](size_t e) { return (e + 63) & ~(size_t)63; };
+    size_t need = 0;
+    for (Request* r : round)
+      if (!r->res) need += seg((size_t)r->n + 1) + seg((size_t)std::max<int64_t>(r->m, 1));
+    if (need > stage_cap) {
+      cudaFree(stage);
+      stage = nullptr;
+      stage_cap = 0;
+      const size_t want = need + need / 4;
+      if (cudaMalloc(&stage, sizeof(int32_t) * want) == cudaSuccess) {
+        stage_cap = want;
+      } else {
+        glp::set_error("staging a round's host CSRs: out of device memory");
+        rc = GLP_ENOMEM;
+      }
+    }
+    size_t at = 0;
+    bool uploaded = false;
+    for (size_t i = 0; i < G; ++i) {
       Request* r = round[i];
       ns[i] = r->n;
       ms[i] = r->m;
@@ -371,34 +418,37 @@ void batch_worker(glp_server* s) {
         cols[i] = r->res->d_cols;
         continue;
       }
-      int32_t *d_o = nullptr, *d_c = nullptr;
-      if (cudaMalloc(&d_o, sizeof(int32_t) * ((size_t)r->n + 1)) != cudaSuccess ||
-          cudaMalloc(&d_c, sizeof(int32_t) * (size_t)std::max<int64_t>(r->m, 1)) != cudaSuccess ||
-          cudaMemcpyAsync(d_o, r->offsets, sizeof(int32_t) * ((size_t)r->n + 1), cudaMemcpyHostToDevice, up) !=
+      if (rc != GLP_OK) continue;
+      int32_t* d_o = stage + at;
+      at += seg((size_t)r->n + 1);
+      int32_t* d_c = stage + at;
+      at += seg((size_t)std::max<int64_t>(r->m, 1));
+      if (cudaMemcpyAsync(d_o, r->offsets, sizeof(int32_t) * ((size_t)r->n + 1), cudaMemcpyHostToDevice, up) !=
               cudaSuccess ||
           (r->m &&
            cudaMemcpyAsync(d_c, r->cols, sizeof(int32_t) * (size_t)r->m, cudaMemcpyHostToDevice, up) != cudaSuccess)) {
         glp::set_error("uploading a request's CSR failed");
         rc = GLP_ECUDA;
       }
-      temps.push_back(d_o);
-      temps.push_back(d_c);
+      uploaded = true;
       offs[i] = d_o;
       cols[i] = d_c;
     }
-    if (rc == GLP_OK && !temps.empty() && cudaStreamSynchronize(up) != cudaSuccess) {
+    if (rc == GLP_OK && uploaded && cudaStreamSynchronize(up) != cudaSuccess) {
       glp::set_error("uploading a request's CSR failed");
       rc = GLP_ECUDA;
     }
-    if (rc == GLP_OK)
-      rc = b ? glp_batch_repack(b, (int32_t)G, offs.data(), cols.data(), ns.data(), ms.data(), 1, its.data())
-             : glp_batch_create_ex((int32_t)G, offs.data(), cols.data(), ns.data(), ms.data(), 1, its.data(), &b);
+    if (rc == GLP_OK && b) {
+      rc = glp_batch_repack(b, (int32_t)G, offs.data(), cols.data(), ns.data(), ms.data(), 1, its.data());
+    } else if (rc == GLP_OK) {
+      rc = glp_batch_create_ex((int32_t)G, offs.data(), cols.data(), ns.data(), ms.data(), 1, its.data(), &b);
+      if (rc == GLP_OK) rc = glp::batch_set_stream_priority(b, s->high_priority);
+    }
     if (rc == GLP_OK) {
       packed.resize((size_t)std::max<int64_t>(total, 1));
       rc = glp_batch_run(b, nullptr, GLP_BATCH_OWN_ITERATIONS, packed.data(), 0, nullptr, nullptr);
     }
     const std::string err = rc ? glp_last_error() : std::string();
-    for (void* t : temps) cudaFree(t);
     s->rounds++;
     int64_t base = 0;
     for (Request* r : round) {
@@ -434,6 +484,7 @@ int submit_request(glp_server* s, std::unique_ptr<Request> r, int64_t* id) {
   // about 1e10 edge visits per second for a one-graph solve, plus a fixed part
   const int64_t iters = (int64_t)r->niter * (r->method == GLP_METHOD_LAYERED ? std::max(1, r->params.nlayers) : 1);
   r->cost_s = 1e-3 + (double)(r->m + r->n) * (double)iters * 1e-10;
+  r->short_job = !r->batched && s->cfg.short_job_us > 0 && r->cost_s * 1e6 < (double)s->cfg.short_job_us;
   if (r->bytes > s->cfg.hbm_budget_bytes) {
     glp::set_error("request needs about %lld bytes, above the server's HBM budget", (long long)r->bytes);
     return GLP_ENOMEM;
@@ -490,6 +541,7 @@ int glp_server_config_default(glp_server_config* c) {
   c->max_batch_graphs = 4096;
   c->plain_workers = 1;
   c->batch_max_vertices = 1 << 22;
+  c->short_job_us = 20000;
   return GLP_OK;
 }
 
@@ -522,11 +574,15 @@ int glp_server_start(const glp_server_config* cfg, glp_server** out) {
     set_error("device %d does not exist", c.device);
     return GLP_EINVAL;
   }
+  if (c.short_job_us == 0) c.short_job_us = 20000;
   std::unique_ptr<glp_server> s(new glp_server());
   s->cfg = c;
   s->t0 = Clock::now();
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) s->high_priority = greatest;
   s->threads.emplace_back(batch_worker, s.get());
-  for (int i = 0; i < c.plain_workers; ++i) s->threads.emplace_back(plain_worker, s.get());
+  for (int i = 0; i < c.plain_workers; ++i) s->threads.emplace_back(plain_worker, s.get(), false);
+  if (c.short_job_us > 0) s->threads.emplace_back(plain_worker, s.get(), true);
   *out = s.release();
   return GLP_OK;
 }
@@ -811,7 +867,7 @@ int glp_server_cancel(glp_server* s, int64_t id) {
       r->stats.status = GLP_ECANCELED;
       release_graph_locked(s, r->res);
       r->res = nullptr;
-    } else if (take(s->batch_q) || take(s->plain_q)) {
+    } else if (take(s->batch_q) || take(s->plain_q) || take(s->short_q)) {
       finish_locked(s, r, GLP_ECANCELED, "cancelled before it started");
     }
     // otherwise it is running: its worker sees r->cancel

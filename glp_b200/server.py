@@ -25,7 +25,8 @@ class ServerConfig(C.Structure):
         ("max_batch_graphs", C.c_int32),
         ("plain_workers", C.c_int32),
         ("batch_max_vertices", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("short_job_us", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -54,7 +55,8 @@ class Request:
 
 class Server:
     def __init__(self, hbm_budget_bytes: int | None = None, max_batch_graphs: int | None = None,
-                 plain_workers: int | None = None, batch_max_vertices: int | None = None, device: int = -1):
+                 plain_workers: int | None = None, batch_max_vertices: int | None = None, device: int = -1,
+                 short_job_us: int | None = None):
         self._lib = _lib.load()
         cfg = ServerConfig()
         _lib.check(self._lib.glp_server_config_default(C.byref(cfg)))
@@ -67,6 +69,8 @@ class Server:
             cfg.plain_workers = plain_workers
         if batch_max_vertices is not None:
             cfg.batch_max_vertices = batch_max_vertices
+        if short_job_us is not None:
+            cfg.short_job_us = short_job_us
         h = C.c_void_p()
         _lib.check(self._lib.glp_server_start(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -369,7 +369,9 @@ int glp_batch_tune(glp_batch* b, int32_t probe_iters, glp_params* best, float* t
  * batched kernel, each round taking every such request admitted so far
  * (continuous batching at round granularity); the rest run as one-graph
  * solves on plain_workers threads whose device work overlaps the rounds,
- * shortest expected job first (aged by waiting time).
+ * shortest expected job first (aged by waiting time); short one-graph
+ * solves (short_job_us) have a worker of their own.  The rounds and the
+ * short solves run on streams of the device's highest priority.
  * Every result equals glp_run of that request alone. */
 typedef struct glp_server glp_server;
 typedef struct glp_server_config {
@@ -379,7 +381,12 @@ typedef struct glp_server_config {
   int32_t max_batch_graphs;    /* requests per batched round (default 4096) */
   int32_t plain_workers;       /* concurrent one-graph solves (default 1) */
   int32_t batch_max_vertices;  /* larger graphs take the one-graph path (default 2^22) */
-  int32_t reserved[8];
+  int32_t short_job_us;        /* one-graph requests expected to take less than this
+                                  (default 0: 20000 us; -1: none) run on a worker of
+                                  their own at the device's highest stream priority,
+                                  next to the batched rounds, instead of queueing
+                                  behind long solves */
+  int32_t reserved[7];
 } glp_server_config;
 typedef struct glp_request_stats {
   double submit_s, admit_s, start_s, done_s; /* seconds since the server started */

@@ -131,6 +131,38 @@ def test_layered_weighted():
     np.testing.assert_array_equal(res.vol, vol)
 
 
+@pytest.mark.parametrize("case", ["rmat12", "planted20k"])
+def test_layered_wide_scores(case):
+    """Weights and dstar large enough that dstar * (a row's weight sum) passes
+    2^31: the layered steps score in 64 bits (no first-step shortcut, no
+    packed reduction); the same labels and volumes as the oracle."""
+    off, cols = CASES[case]
+    w = graphs.add_weights(from_numpy(off, cols), 1_000_000, seed=12).weights.numpy()
+    cs = np.concatenate([[0], np.cumsum(w, dtype=np.int64)])
+    wsum = (cs[off[1:]] - cs[off[:-1]]).max()
+    assert 65536 * int(wsum) >= 2 ** 31
+    dstar = [65536, 2]  # the second layer fits 32 bits again
+    res, tr = _run_trace(off, cols, _lib.METHOD_LAYERED, 3, w=w, dstar=dstar)
+    lab, vol, otr = O.layered_run(off, cols, dstar, 3, w=w, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+    np.testing.assert_array_equal(res.vol, vol)
+
+
+@pytest.mark.parametrize("case", ["rmat12", "planted20k", "star_ring_3000"])
+def test_layered_rows_not_ascending(case):
+    """Rows listed in descending column order: the layer's first step counts
+    like any other (the streaming shortcut needs strictly ascending rows)."""
+    off, cols = CASES[case]
+    rev = cols.copy()
+    for v in range(len(off) - 1):
+        rev[off[v]:off[v + 1]] = cols[off[v]:off[v + 1]][::-1]
+    dstar = [2, 5, 17]
+    res, tr = _run_trace(off, rev, _lib.METHOD_LAYERED, 3, dstar=dstar)
+    lab, vol, otr = O.layered_run(off, rev, dstar, 3, trace=True)
+    np.testing.assert_array_equal(tr, otr)
+    np.testing.assert_array_equal(res.vol, vol)
+
+
 @pytest.mark.parametrize("tier", ["default", "small_hubs"])
 @pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_3000", "planted20k", "path"])
 def test_slpa(case, tier):
@@ -432,7 +464,7 @@ def test_two_step_cycle_stop_is_exact(scale):
 @pytest.mark.parametrize("pf", [0, -1])
 @pytest.mark.parametrize("case", ["rmat14", "ladder", "planted20k", "star_ring_3000"])
 def test_prefetching_tier_kernels_keep_labels(case, pf):
-    """The mid and big tiers with (default) and without the next-vertex
+    """The mid tier with (default) and without the next-vertex
     prefetch give the oracle's labels after every iteration, in full-count
     steps and in majority / frontier steps."""
     off, cols = CASES[case]

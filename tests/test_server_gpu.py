@@ -178,6 +178,32 @@ def _long_layered():
     return graphs.rmat(18, 16, seed=131), _lib.METHOD_LAYERED, 200, make_params(dstar=[2, 3, 5, 9, 17])
 
 
+@pytest.mark.parametrize("short_us", [0, -1])
+def test_short_jobs_do_not_wait_behind_a_long_solve(short_us):
+    """A small layered solve submitted while a long one runs: with the short
+    lane (default) it runs at once on its own worker and finishes first;
+    without it (short_job_us = -1) it waits for the only plain worker.  The
+    result is the solo result either way."""
+    big, m, k, p = _long_layered()
+    small = graphs.planted(20000, 8, 10.0, 2.0, seed=150)
+    sp = make_params(dstar=[2, 3, 5])
+    with Server(plain_workers=1, short_job_us=short_us) as s:
+        gid = s.add_graph(big)
+        h_big = s.submit_graph(gid, m, k, p)
+        t0 = time.perf_counter()
+        while s.stats(h_big)[1]["start_s"] == 0.0 and time.perf_counter() - t0 < 30:
+            time.sleep(0.001)
+        h_small = s.submit(small, _lib.METHOD_LAYERED, 10, sp)
+        st_small = s.wait(h_small, 120000)
+        st_big = s.wait(h_big, 120000)
+    np.testing.assert_array_equal(h_small.labels, _solo(small, _lib.METHOD_LAYERED, 10, sp))
+    assert st_small["path"] == 0 and st_big["status"] == 0
+    if short_us == 0:
+        assert st_small["done_s"] < st_big["done_s"]
+    else:
+        assert st_small["start_s"] >= st_big["done_s"]
+
+
 def test_cancel_before_admission_and_before_start():
     """Host-side failure handling: a tiny budget keeps requests pending; a
     cancelled pending request ends with GLP_ECANCELED without running, and
