@@ -821,8 +821,9 @@ static int ensure_sorted(glp_graph* g) {
 // ascending: unweighted, the row's last column (k_first_step); weighted, the
 // row's largest (weight, label), per tier: a thread per vertex up to degree
 // 32, a warp per mid vertex, a block per big vertex and hub.
-// Per tier, the neighbour of largest key (a thread per vertex up to degree
-// 32, a warp per mid vertex, a block per big vertex and hub).
+// Per tier, the neighbour of largest key: a thread per vertex up to degree
+// 32 (eight loads in flight), a warp per mid vertex, a block per big vertex
+// and hub.
 template <class K>
 static int launch_first_keyed(const DevicePlan& p, const StepArgs& a, const K& key, cudaStream_t s,
                               int64_t* launches) {
@@ -1024,6 +1025,17 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
   int32_t* vol_w = g->d_vol[1];
   GLP_CUDA(cudaMemsetAsync(vol_r, 0, sizeof(int32_t) * g->n, c.s));
   GLP_CUDA(cudaMemsetAsync(vol_w, 0, sizeof(int32_t) * g->n, c.s));
+  // 32-bit layers gather (label, volume) pairs, rebuilt after every step
+  bool any_narrow = false;
+  for (int32_t layer = 0; layer < p.nlayers; ++layer)
+    any_narrow = any_narrow || (int64_t)p.dstar[layer] * g->max_wsum + g->n < 2147483648LL;
+  if (any_narrow && (g->lv_elems < g->n || !g->d_lv)) {
+    dev_free(g->d_lv);
+    g->d_lv = nullptr;
+    GLP_CUDA(dev_alloc(&g->d_lv, sizeof(int2) * std::max(g->n, 1)));
+    g->lv_elems = g->n;
+  }
+  const unsigned lv_grid = (unsigned)std::min<int64_t>(cdiv(std::max(g->n, 1), 256), device_sms() * 16);
   int32_t step = 0;
   int32_t* final_lab = g->d_lab[0];
   for (int32_t layer = 0; layer < p.nlayers; ++layer) {
@@ -1031,11 +1043,13 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
     // most a row's weight sum, a volume at most n
     const bool narrow = (int64_t)p.dstar[layer] * g->max_wsum + g->n < 2147483648LL;
     if ((rc = init_labels(c))) return rc;
+    bool lv_fresh = false;  // d_lv holds (labels, vol_r) of this step's input
     for (int32_t it = 0; it < niter; ++it, ++step) {
       if (step > 0) {
         std::swap(vol_r, vol_w);
         GLP_CUDA(cudaMemsetAsync(vol_w, 0, sizeof(int32_t) * g->n, c.s));
       }
+      const bool first = it == 0 && narrow && g->rows_sorted == 1;
       int32_t* lin = g->d_lab[it & 1];
       int32_t* lout = g->d_lab[(it + 1) & 1];
       set_l2_window(c, lin);
@@ -1047,14 +1061,18 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       L.prev_changed = it > 0 ? g->d_changed + step - 1 : nullptr;
       L.allow_majority = 0;
       L.allow_frontier = 0;
-      if (it == 0 && narrow && g->rows_sorted == 1) {
+      if (first) {
         // labels = ids and no repeated neighbour: every label occurs once, so
         // the step is a streaming maximum of dstar*w - vol_r[neighbour]
         if (L.ev) GLP_CUDA(cudaEventRecord(L.ev[16], c.s));
         rc = launch_first_keyed(g->plan, a, FirstKeyLayered<W>{vol_r, p.dstar[layer]}, c.s, &c.launches);
         if (!rc && L.ev) GLP_CUDA(cudaEventRecord(L.ev[17], c.s));
       } else if (narrow) {
-        rc = launch_step<W>(L, a, ScoreLayered32{vol_r, p.dstar[layer]}, &c.launches);
+        if (!lv_fresh) {  // the layer's first step counted: pairs of the reset labels
+          k_label_volumes<<<lv_grid, 256, 0, c.s>>>(lin, vol_r, g->n, g->d_lv);
+          ++c.launches;
+        }
+        rc = launch_step<W>(L, a, ScoreLayered32{vol_r, p.dstar[layer], g->d_lv}, &c.launches);
       } else {
         rc = launch_step<W>(L, a, ScoreLayered{vol_r, (int64_t)p.dstar[layer]}, &c.launches);
       }
@@ -1062,6 +1080,12 @@ static int run_layered(RunCtx& c, const glp_params& p, int32_t niter) {
       if ((rc = c.aux_mark(0))) return rc;
       k_histogram<<<(unsigned)cdiv(g->n, 256), 256, 0, c.s>>>(lout, g->n, vol_w);
       ++c.launches;
+      // the next step of this layer reads (lout, vol_w) pairs
+      lv_fresh = narrow && it + 1 < niter && g->n > 0;
+      if (lv_fresh) {
+        k_label_volumes<<<lv_grid, 256, 0, c.s>>>(lout, vol_w, g->n, g->d_lv);
+        ++c.launches;
+      }
       if ((rc = c.aux_mark(1))) return rc;
       GLP_CUDA(cudaGetLastError());
       if ((rc = after_iter(c, step, lout))) return rc;
@@ -1529,6 +1553,7 @@ void glp_graph_destroy(glp_graph* g) {
   dev_free(g->d_lab[1]);
   dev_free(g->d_vol[0]);
   dev_free(g->d_vol[1]);
+  dev_free(g->d_lv);
   dev_free(g->d_spoken);
   dev_free(g->d_mem);
   dev_free(g->d_changed);

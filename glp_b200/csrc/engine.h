@@ -151,6 +151,8 @@ struct glp_graph {
   int deg_sorted = 0;    // 1: degrees never increase along the vertex ids
   uint32_t mid_wsum = 0;  // weighted: largest weight sum of a vertex of degree <= kMidCap / 2
   uint32_t max_wsum = 0;  // largest weight sum of a row (unweighted: the largest degree)
+  int2* d_lv = nullptr;   // layered: (label, volume of the label) per vertex
+  int64_t lv_elems = 0;
   cudaStream_t last_stream = nullptr;  // the stream of the latest run
   const volatile int32_t* cancel = nullptr;  // glp_graph_set_cancel_flag: non-zero stops a run
   uint32_t epoch = 0;  // frontier mark of the last step

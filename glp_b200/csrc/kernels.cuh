@@ -195,6 +195,11 @@ struct ScoreClassic {
   static __device__ __forceinline__ unsigned long long pack(const Best& b) {
     return ((unsigned long long)b.s << 32) | (uint32_t)b.l;
   }
+  // the label of neighbour c (and, for scores that carry it, its volume)
+  static constexpr bool kLV = false;
+  __device__ __forceinline__ void load(const StepArgs& a, int32_t c, int32_t& lab, int32_t&) const {
+    lab = ld_label(a.lin + c);
+  }
 };
 
 // score(l, k) for layered LP: dstar*k - vol_r[l] (kernel.cuh:2575-2600).
@@ -217,6 +222,10 @@ struct ScoreLayered {
   // the largest score a label of count <= k can have (volumes are >= 0)
   __device__ __forceinline__ int64_t bound(uint32_t k) const { return dstar * (int64_t)k; }
   static __device__ __forceinline__ unsigned long long pack(const Best&) { return 0ull; }  // not packed
+  static constexpr bool kLV = false;
+  __device__ __forceinline__ void load(const StepArgs& a, int32_t c, int32_t& lab, int32_t&) const {
+    lab = ld_label(a.lin + c);
+  }
 };
 
 // The same layered score in 32-bit arithmetic, for graphs where every score
@@ -226,14 +235,23 @@ struct ScoreLayered {
 // ((score + 2^31) << 32 | label, monotone in (score, label)), so the big tier
 // reduces with one shared atomicMax and the unweighted tables take 16-bit
 // counts, as in classic LP: fewer registers and smaller tables, more blocks
-// per SM.
+// per SM.  The mid and big tiers read each neighbour's (label, volume of
+// that label) as one 8-byte pair from lv, which the step before wrote
+// (k_label_volumes): one random gather per entry instead of two.
 struct ScoreLayered32 {
   static constexpr bool kMajority = false;
   static constexpr bool kPacked = true;
   static constexpr bool kScan = true;
   static constexpr int kSMThreads = 1536;  // 40 registers a thread: 32 would spill
+  static constexpr bool kLV = true;
   const int32_t* vol;
   int32_t dstar;
+  const int2* lv;  // [n] (label of v, vol[label of v]); .x equals lin[v]
+  __device__ __forceinline__ void load(const StepArgs&, int32_t c, int32_t& lab, int32_t& vl) const {
+    const int2 x = __ldg(lv + c);
+    lab = x.x;
+    vl = x.y;
+  }
   __device__ __forceinline__ int64_t operator()(int32_t l, uint32_t k) const {
     return (int64_t)(dstar * (int32_t)k - __ldg(vol + l));
   }
@@ -386,9 +404,10 @@ __global__ void __launch_bounds__(256) k_group(StepArgs a, TierWork tw, S score)
 // __match_any_sync costs a round per distinct value on B200, while a 32-bit
 // shared atomicAdd stays cheap under moderate contention.  Called by all
 // lanes of the warp.
-template <bool W, class S, class Ins>
+// VIN: vl_in is the volume of lab, loaded with it (S::load of an S::kLV score).
+template <bool W, bool VIN = false, class S, class Ins>
 __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, const S& score, const Ins& insert,
-                                            Best& best, bool& fail, bool scan = false) {
+                                            Best& best, bool& fail, bool scan = false, int32_t vl_in = 0) {
   const int lane = threadIdx.x & 31;
   const int32_t l0 = __shfl_sync(kFull, has ? lab : -1, 0);
   const uint32_t m0 = __ballot_sync(kFull, has && lab == l0);
@@ -399,7 +418,8 @@ __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, 
     else if (has && lab == l0) has = false;  // counted by lane 0
   }
   if (!has) return;
-  const int32_t vl = (S::kScan && !scan) ? score.vol_of(lab) : 0;  // in flight during the insert
+  // the volume (S::kLV: loaded with the label) is in flight during the insert
+  const int32_t vl = (S::kScan && !scan) ? (VIN ? vl_in : score.vol_of(lab)) : 0;
   const uint32_t tot = insert((uint32_t)lab + 1u, k);
   if (tot == kNoSlot) {
     fail = true;
@@ -524,7 +544,7 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
   uint32_t* vv = svals[warp];
   // batch loader: columns (and weights) of entries j0 + 32q + lane below e,
   // then their labels (-1 past the row)
-  auto load_batch = [&](int32_t j0, int32_t e, int32_t (&lab)[4], uint32_t (&wt)[4]) {
+  auto load_batch = [&](int32_t j0, int32_t e, int32_t (&lab)[4], uint32_t (&wt)[4], int32_t (&vl)[4]) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int32_t j = j0 + 32 * q + lane;
@@ -533,10 +553,10 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-      if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
+      if (lab[q] >= 0) score.load(a, lab[q], lab[q], vl[q]);
   };
   int32_t pv = 0, pb = 0, pe = 0;  // PF: the next vertex and its first batch
-  int32_t plab[4];
+  int32_t plab[4], pvl[4];
   uint32_t pwt[4];
   auto prefetch = [&](int32_t idx) {
     pb = pe = 0;
@@ -545,13 +565,13 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
       pb = a.off[pv];
       pe = a.off[pv + 1];
     }
-    load_batch(pb, pe, plab, pwt);
+    load_batch(pb, pe, plab, pwt, pvl);
   };
   int32_t i = blockIdx.x * NW + warp;
   if (PF) prefetch(i);
   for (; i < nwork; i += stride) {
     int32_t v, b, e;
-    int32_t lab0[4];
+    int32_t lab0[4], vl0[4];
     uint32_t wt0[4];
     if (PF) {
       v = pv;
@@ -561,6 +581,7 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
       for (int q = 0; q < 4; ++q) {
         lab0[q] = plab[q];
         wt0[q] = pwt[q];
+        vl0[q] = pvl[q];
       }
       prefetch(i + stride);  // in flight while this vertex is counted
     } else {
@@ -578,20 +599,21 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
       return table_insert_bounded<C16>(kk, vv, cap - 1, key, k, cap, nullptr, nullptr);
     };
     for (int32_t j0 = b; j0 < e; j0 += 128) {
-      int32_t lab[4];
+      int32_t lab[4], vl[4];
       uint32_t wt[4];
       if (PF && j0 == b) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           lab[q] = lab0[q];
           wt[q] = wt0[q];
+          vl[q] = vl0[q];
         }
       } else {
-        load_batch(j0, e, lab, wt);
+        load_batch(j0, e, lab, wt, vl);
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + 32 * q < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
+        if (j0 + 32 * q < e) count_chunk<W, S::kLV>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, vl[q]);
     }
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {
@@ -707,7 +729,7 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
       return table_insert_bounded<C16>(keys, vals, cap - 1, key, k, cap, nullptr, nullptr);
     };
     for (int32_t j0 = b + warp * 32; j0 < e; j0 += 4 * NT) {
-      int32_t lab[4];
+      int32_t lab[4], vl[4];
       uint32_t wt[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -717,10 +739,10 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (lab[q] >= 0) lab[q] = ld_label(a.lin + lab[q]);
+        if (lab[q] >= 0) score.load(a, lab[q], lab[q], vl[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + q * NT < e) count_chunk<W>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan);
+        if (j0 + q * NT < e) count_chunk<W, S::kLV>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, vl[q]);
     }
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {  // block-uniform
@@ -1105,15 +1127,16 @@ struct FirstKeyW {
     return ((unsigned long long)(uint32_t)a.w[j] << 32) | (uint32_t)a.lin[a.cols[j]];
   }
 };
-// Layered LP at the start of a layer: every label occurs once, so label l of
-// edge weight k (1 unweighted) scores dstar*k - vol_r[l], in 32 bits (the host
-// checks the range) and packed as ScoreLayered32::pack does.
+// Layered LP at the start of a layer: every label is its vertex id and
+// occurs once, so neighbour c of edge weight k (1 unweighted) scores
+// dstar*k - vol_r[c], in 32 bits (the host checks the range) and packed as
+// ScoreLayered32::pack does.  No label gather: the label is the column.
 template <bool W>
 struct FirstKeyLayered {
   const int32_t* vol;
   int32_t dstar;
   __device__ __forceinline__ unsigned long long operator()(const StepArgs& a, int32_t j) const {
-    const int32_t l = ld_label(a.lin + ld_stream(a.cols + j));
+    const int32_t l = ld_stream(a.cols + j);
     const int32_t k = W ? ld_stream(a.w + j) : 1;
     const int32_t sc = dstar * k - __ldg(vol + l);
     return ((unsigned long long)((uint32_t)sc ^ 0x80000000u) << 32) | (uint32_t)l;
@@ -1130,7 +1153,16 @@ __global__ void __launch_bounds__(256) k_first_step_w(StepArgs a, Verts vs, K ke
     if (i < vs.n) {
       v = vs[i];
       const int32_t b = a.off[v], e = a.off[v + 1];
-      for (int32_t j = b + lane; j < e; j += G) best = max(best, key(a, j));
+      if (G == 1) {
+        // eight entries a round, their loads in flight together
+        for (int32_t j0 = b; j0 < e; j0 += 8) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (j0 + q < e) best = max(best, key(a, j0 + q));
+        }
+      } else {
+        for (int32_t j = b + lane; j < e; j += G) best = max(best, key(a, j));
+      }
     }
 #pragma unroll
     for (int m = G / 2; m >= 1; m >>= 1) best = max(best, __shfl_xor_sync(kFull, best, m));
@@ -1298,6 +1330,16 @@ __global__ void __launch_bounds__(256) k_histogram(const int32_t* __restrict__ l
   if (l < 0) return;
   if (l != l0) atomicAdd(vol + l, 1);
   else if ((threadIdx.x & 31) == 0) atomicAdd(vol + l, __popc(m0));
+}
+
+// lv[v] = (lab[v], vol[lab[v]]): the pairs the next layered step gathers,
+// one 8-byte load per neighbour (ScoreLayered32::load).
+__global__ void __launch_bounds__(256) k_label_volumes(const int32_t* __restrict__ lab, const int32_t* __restrict__ vol,
+                                                       int32_t n, int2* __restrict__ lv) {
+  for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const int32_t l = lab[v];
+    lv[v] = make_int2(l, __ldg(vol + l));
+  }
 }
 
 // ------------------------------------------------------------------- SLPA
