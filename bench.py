@@ -547,7 +547,7 @@ def run_glp(args, ws, rank, local):
         if rank == 0:
             line["suite"] = su
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(_with_summary(line)))
 
 
 # ----------------------------------------------------------------- suite
@@ -679,6 +679,42 @@ def served_requests(count: int, seed: int, device):
         reqs.append({"g": g, "gi": next(k for k, x in enumerate(pool) if x is g), "method": method, "niter": niter,
                      "params": params, "u_gap": u[4]})
     return reqs, pool
+
+
+def _with_summary(line: dict) -> dict:
+    """The line with a compact "summary" right after "config": the figures of
+    the long objects at its end (baselines, parity, batched, served, suite)
+    in a few hundred bytes, so that a reader of a truncated line sees them."""
+    sm = {}
+    cpu, ref = line.get("cpu_baseline"), line.get("reference_gpu_kernels")
+    if isinstance(cpu, dict):
+        sm["cpu_baseline_gteps"] = cpu.get("value")
+    if isinstance(ref, dict):
+        sm["reference_gpu_kernels_gteps"] = ref.get("value")
+    if "parity" in line:
+        sm["parity"] = line["parity"].get("labels_equal_oracle") if isinstance(line["parity"], dict) else None
+    rf = line.get("roofline")
+    if isinstance(rf, dict):
+        sm["roofline_frac"] = rf.get("frac")
+    b = line.get("batched")
+    if isinstance(b, dict):
+        sm["batched_graphs_per_s"] = b.get("value")
+        sm["batched_vs_plain"] = b.get("vs_plain")
+    sv = line.get("served")
+    if isinstance(sv, dict):
+        sm["served"] = [{"rate": r["rate"], "throughput": r["served"]["throughput"],
+                         "sequential_throughput": r["sequential"]["throughput"],
+                         "vs_sequential": r["throughput_vs_sequential"], "p50_ms": r["served"]["p50_ms"],
+                         "sequential_p50_ms": r["sequential"]["p50_ms"]} for r in sv.get("rates", [])]
+    su = line.get("suite")
+    if isinstance(su, dict):
+        sm["suite_gteps"] = {r["workload"]: r["gteps_per_iter"] for r in su.get("runs", [])}
+    out = {}
+    for k, v in line.items():
+        out[k] = v
+        if k == "config":
+            out["summary"] = sm
+    return out
 
 
 def _pct(x, q):

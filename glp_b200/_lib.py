@@ -69,7 +69,8 @@ class Params(C.Structure):
         ("cycle_stop", C.c_int32),
         ("serial_step", C.c_int32),
         ("mid_prefetch", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("batch_blocks", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

@@ -563,8 +563,10 @@ struct Config {
   int half = 1;    // degrees 33..64: 16-lane groups (else whole warps)
   unsigned long long barrier_ns = kBarrierLimitNs;  // grid-barrier wait limit
   int skip_cta = 0;  // failure tests: 1 + a CTA withholding its first arrival
+  int blocks = 0;    // CTAs of the cooperative grid (0: as many as fit every SM)
   bool operator==(const Config& o) const {
-    return nt == o.nt && tt == o.tt && half == o.half && barrier_ns == o.barrier_ns && skip_cta == o.skip_cta;
+    return nt == o.nt && tt == o.tt && half == o.half && barrier_ns == o.barrier_ns && skip_cta == o.skip_cta &&
+           blocks == o.blocks;
   }
 };
 
@@ -631,7 +633,7 @@ int max_degree_in(const glp_batch* b, int lo, int hi) {  // largest degree d wit
 }
 
 template <int NT>
-int launch_k(glp_batch* b, const BatchArgs& a, size_t smem, cudaStream_t s) {
+int launch_k(glp_batch* b, const BatchArgs& a, size_t smem, cudaStream_t s, int max_blocks) {
   auto kern = k_batch<NT>;
   GLP_BCUDA(raise_smem_limit((const void*)kern, smem));
   int per_sm = 0;
@@ -641,7 +643,10 @@ int launch_k(glp_batch* b, const BatchArgs& a, size_t smem, cudaStream_t s) {
     return GLP_ENOTSUP;
   }
   cudaLaunchConfig_t lc = {};
-  lc.gridDim = dim3((unsigned)(per_sm * b->nsm));
+  // a smaller grid leaves SMs to other work: its CTAs can all become resident
+  // while other kernels still hold the rest of the GPU
+  const int fit = per_sm * b->nsm;
+  lc.gridDim = dim3((unsigned)(max_blocks > 0 ? std::min(max_blocks, fit) : fit));
   lc.blockDim = dim3(NT);
   lc.dynamicSmemBytes = smem;
   lc.stream = s;
@@ -656,8 +661,8 @@ int launch_k(glp_batch* b, const BatchArgs& a, size_t smem, cudaStream_t s) {
 
 int launch_cfg(glp_batch* b, const Config& c, const BatchArgs& a, cudaStream_t s) {
   const size_t smem = std::max<size_t>((size_t)(c.nt / 32) * a.warp_words, 2 * (size_t)a.blk_cap) * sizeof(uint32_t);
-  if (c.nt == 512) return launch_k<512>(b, a, smem, s);
-  if (c.nt == 1024) return launch_k<1024>(b, a, smem, s);
+  if (c.nt == 512) return launch_k<512>(b, a, smem, s, c.blocks);
+  if (c.nt == 1024) return launch_k<1024>(b, a, smem, s, c.blocks);
   set_error("no batch kernel for %d threads per block", c.nt);
   return GLP_EINVAL;
 }
@@ -745,6 +750,7 @@ Config config_from(const glp_batch* b, const glp_params* p) {
     if (p->batch_threads == 512 || p->batch_threads == 1024) c.nt = p->batch_threads;
     c.barrier_ns = p->barrier_limit_us > 0 ? 1000ull * (unsigned long long)p->barrier_limit_us : kBarrierLimitNs;
     c.skip_cta = p->fault_skip_cta > 0 ? p->fault_skip_cta : 0;
+    c.blocks = p->batch_blocks > 0 ? p->batch_blocks : 0;
   }
   return c;
 }

@@ -466,7 +466,7 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   GLP_CUDA(cudaEventRecord(L.fork, s));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[0], L.fork, 0));
   GLP_CUDA(cudaStreamWaitEvent(L.aux[1], L.fork, 0));
-  constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 512, kGroupU = 4;
+  constexpr int kMidNT = 256, kBigNT = 256, kHubNT = 512, kBucketNT = 512;
   if (p.n_hubs) {
     const size_t sm = 2ull * kHubTable * sizeof(uint32_t);
     const size_t sm_hist = (size_t)p.hub.max_nb * sizeof(uint32_t);
@@ -592,8 +592,6 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   }
   if (p.g32.n) {
     if ((rc = mark_on(L.aux[1], 2, 0))) return rc;
-    const int64_t warps = cdiv(p.g32.n, 1 * kGroupU);
-    (void)warps;
     k_tiny<32, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.g32.n, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
         a, work(p.g32, 2, nullptr), score);
     if ((rc = mark_on(L.aux[1], 2, 1))) return rc;
@@ -601,8 +599,6 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
   }
   if (p.g16.n) {
     if ((rc = mark_on(L.aux[1], 1, 0))) return rc;
-    const int64_t warps = cdiv(p.g16.n, 2 * kGroupU);
-    (void)warps;
     k_tiny<16, W, S><<<(unsigned)std::min<int64_t>(cdiv(p.g16.n, 256), kMaxGrid), 256, 0, L.aux[1]>>>(
         a, work(p.g16, 1, nullptr), score);
     if ((rc = mark_on(L.aux[1], 1, 1))) return rc;

@@ -363,12 +363,12 @@ void batch_worker(glp_server* s) {
       const double t = s->now();
       for (Request* r : round) {
         r->stats.start_s = t;
-        r->stats.path = round.size() > 1 ? 1 : 0;
+        r->stats.path = (round.size() > 1 || s->cfg.lone_batched > 0) ? 1 : 0;
         r->stats.batch_graphs = (int32_t)round.size();
       }
     }
     for (int64_t id : stale) one.drop(id);
-    if (round.size() == 1) {
+    if (round.size() == 1 && s->cfg.lone_batched <= 0) {
       one.run(round[0]);
       {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -446,7 +446,13 @@ void batch_worker(glp_server* s) {
     }
     if (rc == GLP_OK) {
       packed.resize((size_t)std::max<int64_t>(total, 1));
-      rc = glp_batch_run(b, nullptr, GLP_BATCH_OWN_ITERATIONS, packed.data(), 0, nullptr, nullptr);
+      // a grid sized to the round (one CTA per 8192 vertices, at least 8):
+      // a small round's CTAs can all become resident while a long one-graph
+      // solve still holds the rest of the GPU
+      glp_params bp;
+      glp_params_default(&bp);
+      bp.batch_blocks = (int32_t)std::max<int64_t>(8, (total + 8191) / 8192);
+      rc = glp_batch_run(b, &bp, GLP_BATCH_OWN_ITERATIONS, packed.data(), 0, nullptr, nullptr);
     }
     const std::string err = rc ? glp_last_error() : std::string();
     s->rounds++;

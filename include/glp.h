@@ -122,7 +122,10 @@ typedef struct glp_params {
   int32_t mid_prefetch;           /* mid tier of unweighted classic steps: 0 (default) loads the next
                                      vertex's first 128 neighbour labels while the current vertex is
                                      counted; -1 loads them in turn */
-  int32_t reserved[7];            /* zero */
+  int32_t batch_blocks;           /* batched runs: at most this many CTAs in the cooperative
+                                     grid (0: as many as fit every SM); a small grid can start
+                                     while other kernels hold part of the GPU */
+  int32_t reserved[6];            /* zero */
 } glp_params;
 
 /* Per-iteration observer (parity checks).  labels is a HOST copy of the
@@ -386,7 +389,9 @@ typedef struct glp_server_config {
                                   their own at the device's highest stream priority,
                                   next to the batched rounds, instead of queueing
                                   behind long solves */
-  int32_t reserved[7];
+  int32_t lone_batched;        /* 1: a round of one request runs in the batched kernel
+                                  like any other (default 0: as a one-graph solve) */
+  int32_t reserved[6];
 } glp_server_config;
 typedef struct glp_request_stats {
   double submit_s, admit_s, start_s, done_s; /* seconds since the server started */

@@ -94,6 +94,19 @@ def test_batch_every_configuration_agrees():
                     np.testing.assert_array_equal(ch, ref_ch)
 
 
+@pytest.mark.parametrize("blocks", [1, 3, 8, 148])
+def test_batch_small_grids_agree(blocks):
+    """batch_blocks caps the cooperative grid: every grid size gives the same
+    labels and change counts (the work is grid-strided)."""
+    gs = _mixed()
+    with Batch(gs) as b:
+        ref, ref_ch = b.run(8)
+        p = make_params(batch_blocks=blocks)
+        lab, ch = b.run(8, p)
+        np.testing.assert_array_equal(lab, ref)
+        np.testing.assert_array_equal(ch, ref_ch)
+
+
 def test_batch_tune_graph_replay_and_device_labels():
     gs = _mixed()
     with Batch(gs) as b:

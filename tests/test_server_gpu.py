@@ -59,6 +59,19 @@ def test_served_results_equal_solo_runs():
     assert info["rounds"] >= 1
 
 
+def test_lone_requests_in_the_batched_kernel_equal_solo_runs():
+    """lone_batched = 1: a round of one request runs in the batched kernel
+    (a grid sized to the round) instead of the one-graph engine; results are
+    the solo results."""
+    reqs = _mix()[:13]  # the small classic requests
+    with Server(lone_batched=1) as s:
+        for g, m, k, p in reqs:  # one at a time: every round holds one request
+            h = s.submit(g, m, k, p)
+            st = s.wait(h, 120000)
+            np.testing.assert_array_equal(h.labels, _solo(g, m, k, p))
+            assert st["path"] == 1 and st["batch_graphs"] == 1
+
+
 def test_requests_arriving_during_a_round_join_a_later_round():
     first = [graphs.planted(60000, 16, 12.0, 2.0, seed=50 + i) for i in range(6)]
     later = [graphs.planted(3000, 6, 9.0, 2.0, seed=60 + i) for i in range(6)]
