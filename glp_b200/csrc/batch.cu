@@ -22,8 +22,14 @@
 //                                   lane held in registers: a strict-majority
 //                                   test of the own label, else a per-warp
 //                                   shared table;
-//   thread tier (1 <= d <= TT)    : a thread per vertex, labels in registers,
-//                                   O(d^2) compares.
+//   thread tier (1 <= d <= TT)    : a thread per vertex, labels sorted in
+//                                   registers (bitonic network), counts read
+//                                   off the runs.
+// Every step also writes a change flag per vertex (1 byte).  Once few labels
+// still change (fewer than N/8 in the previous step), a vertex first reads
+// its neighbours' flags of the previous step: if none changed, its
+// neighbourhood is what it was, so is its label (exact on any CSR); it keeps
+// the label without gathering or counting.
 // Neighbouring entries of the order have similar degrees, so the sweeps are
 // balanced without a work queue.  Steps are separated by a grid
 // barrier; the cooperative launch makes every CTA resident, and the barrier
@@ -77,6 +83,8 @@ struct BatchArgs {
   uint32_t blk_cap;        // table slots of the block tier
   int32_t* lab0;
   int32_t* lab1;
+  uint8_t* chg0;           // [N] changed in the last even / odd step (1) or not (0)
+  uint8_t* chg1;
   unsigned long long* changed;  // [niter]
   unsigned int* bar;
   uint32_t* err;
@@ -152,7 +160,8 @@ __device__ __forceinline__ int32_t graph_of(const int64_t* base, int32_t ng, int
 template <int G, int L>
 __device__ __forceinline__ bool group_vertex(const BatchArgs& a, int32_t v, const int32_t* __restrict__ lin,
                                              int32_t* __restrict__ lout, uint32_t* keys, uint32_t* vals,
-                                             bool majority) {
+                                             bool majority, const uint8_t* __restrict__ fin,
+                                             uint8_t* __restrict__ fout) {
   const int lane = threadIdx.x & 31;
   const int gl = lane & (G - 1);
   const uint32_t gmask = G == 32 ? kFull : (((1u << G) - 1u) << (lane & ~(G - 1)));
@@ -169,18 +178,34 @@ __device__ __forceinline__ bool group_vertex(const BatchArgs& a, int32_t v, cons
     const int32_t j = q * G + gl;
     lab[q] = (q * G < dmax && j < d) ? ld_stream(a.cols + b + j) : -1;
   }
-#pragma unroll
-  for (int q = 0; q < L; ++q)
-    if (lab[q] >= 0) lab[q] = ld_label(lin + lab[q]);
   const int32_t own = v >= 0 ? lin[v] : -1;
   bool done = v < 0;
+  if (fin) {  // no neighbour changed in the previous step: the label stays
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < L; ++q)
+      if (lab[q] >= 0) any = any || fin[lab[q]] != 0;
+    if (!done && !(__ballot_sync(kFull, any) & gmask)) {
+      if (gl == 0) {
+        lout[v] = own;
+        fout[v] = 0;
+      }
+      done = true;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < L; ++q)
+    if (lab[q] >= 0 && !done) lab[q] = ld_label(lin + lab[q]);
   if (majority) {
     uint32_t c = 0;
 #pragma unroll
     for (int q = 0; q < L; ++q)
       if (q * G < dmax) c += __popc(__ballot_sync(kFull, lab[q] >= 0 && lab[q] == own) & gmask);
     if (!done && 2 * c > (uint32_t)d) {  // own label is the unique mode
-      if (gl == 0) lout[v] = own;
+      if (gl == 0) {
+        lout[v] = own;
+        fout[v] = 0;
+      }
       done = true;
     }
   }
@@ -217,7 +242,10 @@ __device__ __forceinline__ bool group_vertex(const BatchArgs& a, int32_t v, cons
   if (fail) atomicOr(a.err, kErrProbe);
   best = group_max<G>(best);
   if (done) return false;
-  if (gl == 0) lout[v] = best.l;
+  if (gl == 0) {
+    lout[v] = best.l;
+    fout[v] = best.l != own;
+  }
   return gl == 0 && best.l != own;
 }
 
@@ -232,7 +260,8 @@ constexpr uint32_t group_slots() {  // pow2(2*G*L)
 template <int NT, int G, int L>
 __device__ __forceinline__ uint32_t sweep_groups(const BatchArgs& a, int64_t lo, int64_t hi,
                                                  const int32_t* __restrict__ lin, int32_t* __restrict__ lout,
-                                                 uint32_t* smem_warp, bool majority) {
+                                                 uint32_t* smem_warp, bool majority, const uint8_t* fin,
+                                                 uint8_t* fout) {
   constexpr int kGroups = 32 / G;
   constexpr uint32_t kSlots = group_slots<G, L>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -244,7 +273,7 @@ __device__ __forceinline__ uint32_t sweep_groups(const BatchArgs& a, int64_t lo,
   for (int64_t i0 = lo + ((int64_t)blockIdx.x * (NT / 32) + warp) * kGroups; i0 < hi; i0 += nw * kGroups) {
     const int64_t i = i0 + grp;
     const int32_t v = i < hi ? a.order[i] : -1;
-    chg += group_vertex<G, L>(a, v, lin, lout, keys, vals, majority) ? 1u : 0u;
+    chg += group_vertex<G, L>(a, v, lin, lout, keys, vals, majority, fin, fout) ? 1u : 0u;
   }
   return chg;
 }
@@ -253,10 +282,22 @@ __device__ __forceinline__ uint32_t sweep_groups(const BatchArgs& a, int64_t lo,
 // thread 0.
 template <int NT>
 __device__ __forceinline__ bool block_vertex(const BatchArgs& a, int32_t v, const int32_t* __restrict__ lin,
-                                             int32_t* __restrict__ lout, uint32_t* smem, Best* red) {
+                                             int32_t* __restrict__ lout, uint32_t* smem, Best* red,
+                                             const uint8_t* __restrict__ fin, uint8_t* __restrict__ fout) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t b = a.off[v];
   const int32_t d = (int32_t)(a.off[v + 1] - b);
+  if (fin) {  // block-uniform: no neighbour changed in the previous step, the label stays
+    bool any = false;
+    for (int32_t j = threadIdx.x; j < d && !any; j += NT) any = fin[ld_stream(a.cols + b + j)] != 0;
+    if (!__syncthreads_or(any)) {
+      if (threadIdx.x == 0) {
+        lout[v] = lin[v];
+        fout[v] = 0;
+      }
+      return false;
+    }
+  }
   const uint32_t cap = pow2_ceil(2u * (uint32_t)d);
   uint32_t* keys = smem;
   uint32_t* vals = smem + cap;
@@ -300,7 +341,10 @@ __device__ __forceinline__ bool block_vertex(const BatchArgs& a, int32_t v, cons
   }
   if (fail) atomicOr(a.err, kErrProbe);
   best = block_max<NT>(best, red);
-  if (threadIdx.x == 0) lout[v] = best.l;
+  if (threadIdx.x == 0) {
+    lout[v] = best.l;
+    fout[v] = best.l != lin[v];
+  }
   return threadIdx.x == 0 && best.l != lin[v];
 }
 
@@ -308,13 +352,25 @@ __device__ __forceinline__ bool block_vertex(const BatchArgs& a, int32_t v, cons
 // counts read off the runs (sort_labels).
 template <int TT>
 __device__ __forceinline__ bool thread_vertex(const BatchArgs& a, int32_t v, const int32_t* __restrict__ lin,
-                                              int32_t* __restrict__ lout) {
+                                              int32_t* __restrict__ lout, const uint8_t* __restrict__ fin,
+                                              uint8_t* __restrict__ fout) {
   const int64_t b = a.off[v];
   const int32_t d = (int32_t)(a.off[v + 1] - b);
   int32_t lab[TT];
   uint32_t one[TT];
 #pragma unroll
   for (int i = 0; i < TT; ++i) lab[i] = i < d ? ld_stream(a.cols + b + i) : -1;
+  if (fin) {  // no neighbour changed in the previous step: the label stays
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < TT; ++i)
+      if (lab[i] >= 0) any = any || fin[lab[i]] != 0;
+    if (!any) {
+      lout[v] = lin[v];
+      fout[v] = 0;
+      return false;
+    }
+  }
 #pragma unroll
   for (int i = 0; i < TT; ++i) lab[i] = lab[i] >= 0 ? ld_label(lin + lab[i]) : INT32_MAX;
   sort_labels<TT, false>(lab, one);
@@ -329,16 +385,19 @@ __device__ __forceinline__ bool thread_vertex(const BatchArgs& a, int32_t v, con
       if (better(c, best)) best = c;
     }
   }
+  const int32_t own = lin[v];
   lout[v] = best.l;
-  return best.l != lin[v];
+  fout[v] = best.l != own;
+  return best.l != own;
 }
 
 template <int NT, int TT>
 __device__ __forceinline__ uint32_t sweep_threads(const BatchArgs& a, int64_t lo, int64_t hi,
-                                                  const int32_t* __restrict__ lin, int32_t* __restrict__ lout) {
+                                                  const int32_t* __restrict__ lin, int32_t* __restrict__ lout,
+                                                  const uint8_t* fin, uint8_t* fout) {
   uint32_t chg = 0;
   for (int64_t i = lo + (int64_t)blockIdx.x * NT + threadIdx.x; i < hi; i += (int64_t)gridDim.x * NT)
-    chg += thread_vertex<TT>(a, a.order[i], lin, lout) ? 1u : 0u;
+    chg += thread_vertex<TT>(a, a.order[i], lin, lout, fin, fout) ? 1u : 0u;
   return chg;
 }
 
@@ -386,6 +445,8 @@ __global__ void __launch_bounds__(NT) k_batch(BatchArgs a) {
         chg += nxt != own;
       }
       a.lab1[v] = nxt;
+      a.chg0[v] = nxt != own;  // the first step's flags (none without it)
+      a.chg1[v] = 0;
       if (nxt != own) {  // count it only for graphs that run a step
         int c = 0;
         while (c + 1 < a.nclass && v >= a.class_v[c + 1]) ++c;
@@ -403,23 +464,27 @@ __global__ void __launch_bounds__(NT) k_batch(BatchArgs a) {
     int32_t* lout = (it & 1) ? a.lab0 : a.lab1;
     // a vertex's own label decides it when it holds a strict majority; worth
     // testing once few labels still change
-    const bool majority =
-        it > 0 && *(volatile unsigned long long*)(a.changed + it - 1) < (unsigned long long)(a.n / 4);
+    const unsigned long long prev = it > 0 ? *(volatile unsigned long long*)(a.changed + it - 1) : ~0ull;
+    const bool majority = prev < (unsigned long long)(a.n / 4);
+    // the previous step's flags (written by every vertex it counted; the
+    // first step's by the set-up above), once few labels still change
+    const uint8_t* fin = prev < (unsigned long long)(a.n / 8) ? ((it & 1) ? a.chg0 : a.chg1) : nullptr;
+    uint8_t* fout = (it & 1) ? a.chg1 : a.chg0;
     uint32_t chg = 0;
     for (int c = 0; c < a.nclass; ++c) {
       if (it >= a.class_niter[c]) continue;  // this class has finished
       const int64_t* B = a.bstart[c];
       for (int64_t i = B[0] + blockIdx.x; i < B[1]; i += gridDim.x)
-        chg += block_vertex<NT>(a, a.order[i], lin, lout, smem, red) ? 1u : 0u;
-      chg += sweep_groups<NT, 32, 8>(a, B[1], B[2], lin, lout, smem_warp, majority);
-      chg += sweep_groups<NT, 32, 4>(a, B[2], B[3], lin, lout, smem_warp, majority);
-      if (a.mode & kB3Half) chg += sweep_groups<NT, 16, 4>(a, B[3], B[4], lin, lout, smem_warp, majority);
-      else chg += sweep_groups<NT, 32, 2>(a, B[3], B[4], lin, lout, smem_warp, majority);
-      if (a.mode & kB4Threads) chg += sweep_threads<NT, 32>(a, B[4], B[5], lin, lout);
-      else chg += sweep_groups<NT, 8, 4>(a, B[4], B[5], lin, lout, smem_warp, majority);
-      if (a.mode & kB5Threads) chg += sweep_threads<NT, 16>(a, B[5], B[6], lin, lout);
-      else chg += sweep_groups<NT, 4, 4>(a, B[5], B[6], lin, lout, smem_warp, majority);
-      chg += sweep_threads<NT, 8>(a, B[6], B[7], lin, lout);
+        chg += block_vertex<NT>(a, a.order[i], lin, lout, smem, red, fin, fout) ? 1u : 0u;
+      chg += sweep_groups<NT, 32, 8>(a, B[1], B[2], lin, lout, smem_warp, majority, fin, fout);
+      chg += sweep_groups<NT, 32, 4>(a, B[2], B[3], lin, lout, smem_warp, majority, fin, fout);
+      if (a.mode & kB3Half) chg += sweep_groups<NT, 16, 4>(a, B[3], B[4], lin, lout, smem_warp, majority, fin, fout);
+      else chg += sweep_groups<NT, 32, 2>(a, B[3], B[4], lin, lout, smem_warp, majority, fin, fout);
+      if (a.mode & kB4Threads) chg += sweep_threads<NT, 32>(a, B[4], B[5], lin, lout, fin, fout);
+      else chg += sweep_groups<NT, 8, 4>(a, B[4], B[5], lin, lout, smem_warp, majority, fin, fout);
+      if (a.mode & kB5Threads) chg += sweep_threads<NT, 16>(a, B[5], B[6], lin, lout, fin, fout);
+      else chg += sweep_groups<NT, 4, 4>(a, B[5], B[6], lin, lout, smem_warp, majority, fin, fout);
+      chg += sweep_threads<NT, 8>(a, B[6], B[7], lin, lout, fin, fout);
     }
     block_count_add<NT>(a.changed + it, chg, red_u);
     if (it + 1 < a.niter && !grid_barrier(a.bar, ++phase * gridDim.x, a.err, a.barrier_ns)) return;
@@ -601,6 +666,8 @@ struct glp_batch {
   int64_t class_v[9] = {0};
   int64_t bstart[8][9] = {{0}};
   int32_t* d_lab[2] = {nullptr, nullptr};
+  uint8_t* d_chg[2] = {nullptr, nullptr};  // per-vertex change flags of the last even / odd step
+  size_t cap_chg[2] = {0, 0};
   unsigned long long* d_changed = nullptr;
   int32_t changed_cap = 0;
   unsigned int* d_bar = nullptr;
@@ -696,6 +763,8 @@ BatchArgs make_args(glp_batch* b, const Config& c, int32_t niter) {
   a.blk_cap = bdeg ? pow2_host(2u * (uint32_t)bdeg) : 0u;
   a.lab0 = b->d_lab[0];
   a.lab1 = b->d_lab[1];
+  a.chg0 = b->d_chg[0];
+  a.chg1 = b->d_chg[1];
   a.changed = b->d_changed;
   a.bar = b->d_bar;
   a.err = b->d_err;
@@ -856,6 +925,7 @@ int pack(glp_batch* b, int32_t ngraphs, const int32_t* const* offsets, const int
       (rc = grow(&b->d_order, &b->cap_order, (size_t)N)) || (rc = grow(&b->d_vbase, &b->cap_vbase, (size_t)ngraphs + 1)) ||
       (rc = grow(&b->d_ebase, &b->cap_ebase, (size_t)ngraphs + 1)) ||
       (rc = grow(&b->d_lab[0], &b->cap_lab[0], (size_t)N)) || (rc = grow(&b->d_lab[1], &b->cap_lab[1], (size_t)N)) ||
+      (rc = grow(&b->d_chg[0], &b->cap_chg[0], (size_t)N)) || (rc = grow(&b->d_chg[1], &b->cap_chg[1], (size_t)N)) ||
       (rc = grow(&b->d_stage, &b->cap_stage, (size_t)(N + ngraphs + 1))) ||
       (rc = grow(&b->d_counts, &b->cap_counts, (size_t)nblocks * kKeys)) ||
       (rc = grow(&b->d_start, &b->cap_start, (size_t)nblocks * kKeys))) {
@@ -1022,6 +1092,8 @@ void glp_batch_destroy(glp_batch* b) {
   cudaFree(b->d_flags);
   cudaFree(b->d_lab[0]);
   cudaFree(b->d_lab[1]);
+  cudaFree(b->d_chg[0]);
+  cudaFree(b->d_chg[1]);
   cudaFree(b->d_changed);
   cudaFree(b->d_bar);
   cudaFree(b->d_err);

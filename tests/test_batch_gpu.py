@@ -94,6 +94,25 @@ def test_batch_every_configuration_agrees():
                     np.testing.assert_array_equal(ch, ref_ch)
 
 
+def test_batch_change_flags_exact_on_long_and_directed_runs():
+    """Once few labels change, a vertex none of whose neighbours changed
+    keeps its label without counting.  That is exact on any CSR: long runs
+    (40 iterations, most of them in that mode) on symmetric graphs and on a
+    directed one equal the solo runs and the oracle, change counts included."""
+    rng = np.random.default_rng(21)
+    n = 4000
+    adj = [sorted(set(rng.integers(0, n, size=rng.integers(1, 30)).tolist()) - {v}) for v in range(n)]
+    from tests.graphs_fixtures import csr_from_adj
+    off, cols = csr_from_adj(adj)
+    gs = [graphs.planted(5000, 10, 12.0, 1.0, seed=31), graphs.from_numpy(off, cols),
+          graphs.planted(20000, 40, 6.0, 1.5, seed=32), graphs.rmat(12, 16, seed=33)]
+    with Batch(gs) as b:
+        labels, changed = b.run(40)
+        _check(b, gs, 40, labels, changed)
+        assert changed[-1] < sum(g.n for g in gs) // 8  # the flag mode ran
+        np.testing.assert_array_equal(b.split(labels)[1], O.classic_run(off, cols, 40))
+
+
 @pytest.mark.parametrize("blocks", [1, 3, 8, 148])
 def test_batch_small_grids_agree(blocks):
     """batch_blocks caps the cooperative grid: every grid size gives the same
