@@ -185,7 +185,8 @@ __device__ __forceinline__ bool group_vertex(const BatchArgs& a, int32_t v, cons
 #pragma unroll
     for (int q = 0; q < L; ++q)
       if (lab[q] >= 0) any = any || fin[lab[q]] != 0;
-    if (!done && !(__ballot_sync(kFull, any) & gmask)) {
+    const uint32_t group_any = __ballot_sync(kFull, any) & gmask;  // every lane takes part
+    if (!done && !group_any) {
       if (gl == 0) {
         lout[v] = own;
         fout[v] = 0;
