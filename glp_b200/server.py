@@ -26,7 +26,7 @@ class ServerConfig(C.Structure):
         ("plain_workers", C.c_int32),
         ("batch_max_vertices", C.c_int32),
         ("short_job_us", C.c_int32),
-        ("lone_batched", C.c_int32),
+        ("lone_one_graph", C.c_int32),
         ("reserved", C.c_int32 * 6),
     ]
 
@@ -57,7 +57,7 @@ class Request:
 class Server:
     def __init__(self, hbm_budget_bytes: int | None = None, max_batch_graphs: int | None = None,
                  plain_workers: int | None = None, batch_max_vertices: int | None = None, device: int = -1,
-                 short_job_us: int | None = None, lone_batched: int | None = None):
+                 short_job_us: int | None = None, lone_one_graph: int | None = None):
         self._lib = _lib.load()
         cfg = ServerConfig()
         _lib.check(self._lib.glp_server_config_default(C.byref(cfg)))
@@ -72,8 +72,8 @@ class Server:
             cfg.batch_max_vertices = batch_max_vertices
         if short_job_us is not None:
             cfg.short_job_us = short_job_us
-        if lone_batched is not None:
-            cfg.lone_batched = lone_batched
+        if lone_one_graph is not None:
+            cfg.lone_one_graph = lone_one_graph
         h = C.c_void_p()
         _lib.check(self._lib.glp_server_start(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -389,8 +389,9 @@ typedef struct glp_server_config {
                                   their own at the device's highest stream priority,
                                   next to the batched rounds, instead of queueing
                                   behind long solves */
-  int32_t lone_batched;        /* 1: a round of one request runs in the batched kernel
-                                  like any other (default 0: as a one-graph solve) */
+  int32_t lone_one_graph;      /* 1: a round of one request runs as a one-graph solve
+                                  (default 0: in the batched kernel like any round, on
+                                  a grid sized to it) */
   int32_t reserved[6];
 } glp_server_config;
 typedef struct glp_request_stats {

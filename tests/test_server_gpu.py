@@ -59,17 +59,18 @@ def test_served_results_equal_solo_runs():
     assert info["rounds"] >= 1
 
 
-def test_lone_requests_in_the_batched_kernel_equal_solo_runs():
-    """lone_batched = 1: a round of one request runs in the batched kernel
-    (a grid sized to the round) instead of the one-graph engine; results are
-    the solo results."""
+@pytest.mark.parametrize("lone_one_graph", [0, 1])
+def test_lone_requests_equal_solo_runs(lone_one_graph):
+    """A round of one request: by default it runs in the batched kernel (a
+    grid sized to the round); with lone_one_graph = 1 as a one-graph solve.
+    Results are the solo results either way."""
     reqs = _mix()[:13]  # the small classic requests
-    with Server(lone_batched=1) as s:
+    with Server(lone_one_graph=lone_one_graph) as s:
         for g, m, k, p in reqs:  # one at a time: every round holds one request
             h = s.submit(g, m, k, p)
             st = s.wait(h, 120000)
             np.testing.assert_array_equal(h.labels, _solo(g, m, k, p))
-            assert st["path"] == 1 and st["batch_graphs"] == 1
+            assert st["path"] == 1 - lone_one_graph and st["batch_graphs"] == 1
 
 
 def test_requests_arriving_during_a_round_join_a_later_round():
