@@ -368,7 +368,9 @@ def run_glp(args, ws, rank, local):
     dev = torch.device("cuda", local if ws > 1 else 0)
     g, gen_s = make_graph(args.scale, args.seed, dev)
     n, m = g.n, g.m
-    params = make_params()
+    # every iteration's step runs inside the timed region; the engine's
+    # default stop at a two-step cycle (exact, fewer steps) is timed apart
+    params = make_params(cycle_stop=-1)
     handle = Graph(g)
     plan = handle.plan(params)
     labels_dev = torch.empty(n, dtype=torch.int32, device=dev)
@@ -400,13 +402,31 @@ def run_glp(args, ws, rank, local):
     # kernel of a step on one stream (serial_step), so that a tier's CUDA-event
     # time is its kernels' own duration, not a span shared with the tiers
     # running beside it
-    prof_params = make_params(serial_step=1)
+    prof_params = make_params(serial_step=1, cycle_stop=-1)
     prof_runs = []
     for _ in range(PROFILE_RUNS):
         r = handle.run(_lib.METHOD_CLASSIC, args.iters, prof_params, labels_out=labels_dev, stream=sp, profile=True)
         tier_ms += r.tier_ms
         prof_runs.append(r)
     torch.cuda.synchronize(dev)
+    # the engine's default parameters: a run stops stepping once a step ends
+    # in a two-step cycle (the later labelings are the last two in turn)
+    dflt = make_params()
+    for _ in range(args.warmup):
+        handle.run(_lib.METHOD_CLASSIC, args.iters, dflt, labels_out=labels_dev, stream=sp)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    cyc_launches = 0
+    for _ in range(args.steps):
+        r = handle.run(_lib.METHOD_CLASSIC, args.iters, dflt, labels_out=labels_dev, stream=sp)
+        cyc_launches += r.launches
+    c1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    cyc_ms = max_over_ranks(ws, c0.elapsed_time(c1))
+    cyc_value = sum_over_ranks(ws, float(m) * args.iters * args.steps) / (cyc_ms / 1e3) / 1e9
     ms_max = max_over_ranks(ws, ms)
     edges_total = sum_over_ranks(ws, float(m) * args.iters * args.steps)
     value = edges_total / (ms_max / 1e3) / 1e9
@@ -506,12 +526,18 @@ def run_glp(args, ws, rank, local):
             "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic R-MAT (seeded), generated on the GPU",
             "config": workload_config(args, n, m),
-            "step": f"one {args.iters}-iteration run over the device-resident graph",
+            "step": f"one {args.iters}-iteration run over the device-resident graph, every iteration's step run",
             "parallelism": f"replicas{ws}", "graph_gen_s": round(gen_s, 2),
             "e2e": {"value": round(e2e_value, 3), "unit": "GTEPS", "h2d_bytes_per_step": int(4 * (n + 1 + m)),
                     "d2h_bytes_per_step": int(4 * n), "steps": args.e2e_steps, "labels_match_device_run": same,
                     "host_clock_parts": {k: round(v, 2) for k, v in parts.items()}},
             "gpu_launches": int(launches),
+            "with_cycle_stop": {"value": round(cyc_value, 3),
+                                "ms_per_step": round(cyc_ms / args.steps, 3),
+                                "launches_per_run": int(cyc_launches // max(args.steps, 1)),
+                                "launches_per_run_every_step": int(launches // max(args.steps, 1)),
+                                "how": "the engine's default parameters: a run stops stepping once a step ends in "
+                                       "a two-step cycle; the same final labels"},
             "roofline": {"bound": "hbm", "achieved": roof.get("achieved"), "peak": peak, "unit": "GB/s",
                          "frac": roof.get("frac"), "traffic": traffic, "kernel": roof.get("kernel"),
                          "peak_kind": peak_kind, "bytes_per_launch": roof.get("bytes_per_launch"),
@@ -599,7 +625,8 @@ def run_suite(args, ws, rank, local):
             n, m = g.n, g.m
             wb = 4 * m if weighted else 0
             tag = f"{gname}{'-weighted' if weighted else ''}"
-            measure(f"classic-{tag}-20it", g, _lib.METHOD_CLASSIC, 20, None, 8 * m + 12 * n + 4 + wb, 20)
+            measure(f"classic-{tag}-20it", g, _lib.METHOD_CLASSIC, 20, make_params(cycle_stop=-1),
+                    8 * m + 12 * n + 4 + wb, 20)
             measure(f"layered-{tag}-5x10it", g, _lib.METHOD_LAYERED, 10, gammas, 8 * m + 16 * n + 4 + wb, 50)
             del g
             torch.cuda.empty_cache()
@@ -609,7 +636,8 @@ def run_suite(args, ws, rank, local):
     del g
     torch.cuda.empty_cache()
     return {"peak_gbs": peak, "peak_kind": peak_kind, "runs": out,
-            "how": "device time (CUDA events) of 2 runs after 1 warm-up run, graph resident, labels on the device"}
+            "how": "device time (CUDA events) of 2 runs after 1 warm-up run, graph resident, labels on the device; "
+                   "classic runs run every iteration's step (no stop at a two-step cycle)"}
 
 
 def run_one_path(args, ws, rank, local):
@@ -696,6 +724,9 @@ def _with_summary(line: dict) -> dict:
     rf = line.get("roofline")
     if isinstance(rf, dict):
         sm["roofline_frac"] = rf.get("frac")
+    cs = line.get("with_cycle_stop")
+    if isinstance(cs, dict):
+        sm["with_cycle_stop_gteps"] = cs.get("value")
     b = line.get("batched")
     if isinstance(b, dict):
         sm["batched_graphs_per_s"] = b.get("value")
@@ -738,9 +769,16 @@ def run_served(args, ws, rank, local):
     for rate in rates:
         arrivals = np.cumsum([-np.log(max(1e-12, 1.0 - r["u_gap"])) / rate for r in reqs])
         arrivals -= arrivals[0]
-        # served: the pool is resident (uploaded before the stream starts)
+        # served: the pool is resident (uploaded before the stream starts);
+        # one unpaced pass over the requests warms the server (its workers'
+        # cached handles, per-method buffers and batch buffers), as the
+        # sequential engine below is warmed
         with Server() as srv:
             gids = [srv.add_graph(g) for g in pool]
+            warm = [srv.submit_graph(gids[r["gi"]], r["method"], r["niter"], r["params"]) for r in reqs]
+            for h in warm:
+                srv.wait(h)
+            rounds0 = srv.info()["rounds"]
             handles, lags = [], []
             start = time.perf_counter()
             for r, at in zip(reqs, arrivals):
@@ -750,7 +788,7 @@ def run_served(args, ws, rank, local):
                 lags.append(time.perf_counter() - (start + at))
                 handles.append(srv.submit_graph(gids[r["gi"]], r["method"], r["niter"], r["params"]))
             stats = [srv.wait(h) for h in handles]
-            rounds = srv.info()["rounds"]
+            rounds = srv.info()["rounds"] - rounds0
         lat = [(st["done_s"] - st["submit_s"] + lag) * 1e3 for st, lag in zip(stats, lags)]
         span = max(st["done_s"] for st in stats) - min(st["submit_s"] for st in stats)
         served = {"throughput": round(len(reqs) / span, 1), "p50_ms": round(_pct(lat, 50), 2),
@@ -760,6 +798,8 @@ def run_served(args, ws, rank, local):
         # graphs resident (one handle each, created before the stream)
         lat_s, same, service = [], True, []
         resident = [Graph(g) for g in pool]
+        for r in reqs:  # the same unpaced warm-up pass
+            resident[r["gi"]].run(r["method"], r["niter"], r["params"])
         start = time.perf_counter()
         for r, at, h in zip(reqs, arrivals, handles):
             wait = start + at - time.perf_counter()
@@ -803,9 +843,10 @@ def run_served(args, ws, rank, local):
             "unit": "req/s", "requests": len(reqs), "seed": args.serve_seed, "mix": mix, "rates": out,
             "graph_gen_s": round(gen_s, 2),
             "how": "native server, graph pool resident: FIFO admission by a 150 GB HBM budget, small classic "
-                   "requests in rounds of the persistent batched kernel, the rest on one one-graph worker (shortest job "
-                   "first) with cached "
-                   "handles; sequential = one request at a time through glp_run on resident handles"}
+                   "requests in rounds of the persistent batched kernel (grids sized to the round), one-graph "
+                   "requests expected below 20 ms on a short-job worker, the rest on one one-graph worker (shortest "
+                   "job first) with cached handles; sequential = one request at a time through glp_run on resident "
+                   "handles; both warmed by one unpaced pass over the requests before the timed stream"}
 
 
 # ----------------------------------------------------------------- batched

@@ -26,7 +26,8 @@
 //                                   registers (bitonic network), counts read
 //                                   off the runs.
 // Every step also writes a change flag per vertex (1 byte).  Once few labels
-// still change (fewer than N/8 in the previous step), a vertex first reads
+// still change (fewer than frontier_permille, default 10, per 1000 vertices
+// in the previous step), a vertex first reads
 // its neighbours' flags of the previous step: if none changed, its
 // neighbourhood is what it was, so is its label (exact on any CSR); it keeps
 // the label without gathering or counting.
@@ -85,6 +86,7 @@ struct BatchArgs {
   int32_t* lab1;
   uint8_t* chg0;           // [N] changed in the last even / odd step (1) or not (0)
   uint8_t* chg1;
+  uint32_t flag_pm;        // change-flag skips below this many changes per 1000 vertices
   unsigned long long* changed;  // [niter]
   unsigned int* bar;
   uint32_t* err;
@@ -469,7 +471,9 @@ __global__ void __launch_bounds__(NT) k_batch(BatchArgs a) {
     const bool majority = prev < (unsigned long long)(a.n / 4);
     // the previous step's flags (written by every vertex it counted; the
     // first step's by the set-up above), once few labels still change
-    const uint8_t* fin = prev < (unsigned long long)(a.n / 8) ? ((it & 1) ? a.chg0 : a.chg1) : nullptr;
+    const uint8_t* fin =
+        prev * 1000ull < (unsigned long long)a.flag_pm * (unsigned long long)a.n ? ((it & 1) ? a.chg0 : a.chg1)
+                                                                                 : nullptr;
     uint8_t* fout = (it & 1) ? a.chg1 : a.chg0;
     uint32_t chg = 0;
     for (int c = 0; c < a.nclass; ++c) {
@@ -630,9 +634,10 @@ struct Config {
   unsigned long long barrier_ns = kBarrierLimitNs;  // grid-barrier wait limit
   int skip_cta = 0;  // failure tests: 1 + a CTA withholding its first arrival
   int blocks = 0;    // CTAs of the cooperative grid (0: as many as fit every SM)
+  uint32_t flag_pm = 10;  // change-flag skips below this many changes per 1000 vertices (0: never)
   bool operator==(const Config& o) const {
     return nt == o.nt && tt == o.tt && half == o.half && barrier_ns == o.barrier_ns && skip_cta == o.skip_cta &&
-           blocks == o.blocks;
+           blocks == o.blocks && flag_pm == o.flag_pm;
   }
 };
 
@@ -766,6 +771,7 @@ BatchArgs make_args(glp_batch* b, const Config& c, int32_t niter) {
   a.lab1 = b->d_lab[1];
   a.chg0 = b->d_chg[0];
   a.chg1 = b->d_chg[1];
+  a.flag_pm = c.flag_pm;
   a.changed = b->d_changed;
   a.bar = b->d_bar;
   a.err = b->d_err;
@@ -821,6 +827,8 @@ Config config_from(const glp_batch* b, const glp_params* p) {
     c.barrier_ns = p->barrier_limit_us > 0 ? 1000ull * (unsigned long long)p->barrier_limit_us : kBarrierLimitNs;
     c.skip_cta = p->fault_skip_cta > 0 ? p->fault_skip_cta : 0;
     c.blocks = p->batch_blocks > 0 ? p->batch_blocks : 0;
+    c.flag_pm = p->frontier_permille > 0 ? (uint32_t)std::min(p->frontier_permille, 1000)
+                : p->frontier_permille < 0 ? 0u : 10u;
   }
   return c;
 }

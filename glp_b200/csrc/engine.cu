@@ -1918,6 +1918,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.serial = p.serial_step != 0;
   if (p.majority_permille > 0) c.majority_pm = (uint32_t)std::min(p.majority_permille, 1000);
   if (p.frontier_permille > 0) c.frontier_pm = (uint32_t)std::min(p.frontier_permille, 1000);
+  if (p.frontier_permille < 0) c.frontier_pm = 0;  // never
   c.l2_window = p.l2_window != 0;
   c.cycle = !p.async && p.cycle_stop == 0;
   c.mid_prefetch = p.mid_prefetch == 0;

@@ -107,7 +107,9 @@ typedef struct glp_params {
                                      1000 vertices in the previous step, a step first decides the vertices
                                      whose own label holds a strict majority (0 = 500); every mode is exact */
   int32_t frontier_permille;      /* below this many changes per 1000 vertices, only neighbours of changed
-                                     vertices are recomputed (symmetric graphs; 0 = 50) */
+                                     vertices are recomputed (one-graph runs: symmetric graphs; batched
+                                     runs: vertices with a changed neighbour, any CSR; 0 = 50 one-graph,
+                                     10 batched; -1 = never) */
   int32_t l2_window;              /* 1: keep the label array being gathered in L2 through a persisting
                                      access-policy window on the run's streams (off by default) */
   int32_t cycle_stop;             /* classic runs on symmetric graphs: 0 (default) stops running steps

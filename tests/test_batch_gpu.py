@@ -109,8 +109,12 @@ def test_batch_change_flags_exact_on_long_and_directed_runs():
     with Batch(gs) as b:
         labels, changed = b.run(40)
         _check(b, gs, 40, labels, changed)
-        assert changed[-1] < sum(g.n for g in gs) // 8  # the flag mode ran
+        assert changed[-1] * 1000 < 50 * sum(g.n for g in gs)  # a threshold of 50 per mille engages the mode
         np.testing.assert_array_equal(b.split(labels)[1], O.classic_run(off, cols, 40))
+        for pm in (50, -1, 1000):  # from late steps on / never / every step after the first
+            lab, ch = b.run(40, make_params(frontier_permille=pm))
+            np.testing.assert_array_equal(lab, labels, err_msg=f"frontier_permille {pm}")
+            np.testing.assert_array_equal(ch, changed)
 
 
 @pytest.mark.parametrize("blocks", [1, 3, 8, 148])
