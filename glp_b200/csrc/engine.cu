@@ -525,8 +525,8 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     static_assert(kBigParts == 5 && kBigPartThreads[0] == 256 && kBigPartThreads[1] == 256 &&
                       kBigPartThreads[2] == 512 && kBigPartThreads[3] == 1024 && kBigPartThreads[4] == 1024,
                   "the launches below follow kBigPartThreads");
-    // unweighted counts fit 16 bits: from the second range on, the smaller
-    // 16-bit tables (and S::kSMThreads threads per SM) fit more blocks
+    // unweighted counts fit 16 bits: the claim-first 16-bit tables (and
+    // S::kSMThreads threads per SM) fit more blocks
     constexpr bool k16 = !W && S::kPacked;
     for (int r = 0; r < kBigParts; ++r) {
       const Verts& vs = p.big_part[r];
@@ -534,9 +534,9 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       const TierWork tw{vs, none, none, 1};
       const size_t smr = 4ull * kBigPartMax[r] * sizeof(uint32_t);
       const unsigned grid = (unsigned)std::min<int64_t>(vs.n, kMaxGrid);
-      if (k16 && r > 0 && r < kBigParts - 1) {
+      if (k16 && r < kBigParts - 1) {
         const size_t sm16 = 12ull * kBigPartMax[r];  // 2*max slots of 4 + 2 bytes
-        if (r == 1) {
+        if (r <= 1) {
           k_big<256, false, S, true><<<grid, 256, sm16, s>>>(a, tw, score);
         } else if (r == 2) {
           if ((rc = allow_smem(k_big<512, false, S, true>, sm16))) return rc;
@@ -553,10 +553,10 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       } else if (r == 3) {
         if ((rc = allow_smem(k_big<1024, W, S>, smr))) return rc;
         k_big<1024, W, S><<<grid, 1024, smr, s>>>(a, tw, score);
-      } else if constexpr (!W) {  // the 16-bit range: unweighted graphs only
+      } else if constexpr (!W) {  // the 16-bit range: unweighted graphs only, load-first
         const size_t sm16 = (size_t)kBig16Slots * 6;
-        if ((rc = allow_smem(k_big<1024, false, S, true>, sm16))) return rc;
-        k_big<1024, false, S, true><<<grid, 1024, sm16, s>>>(a, tw, score);
+        if ((rc = allow_smem(k_big<1024, false, S, true, false>, sm16))) return rc;
+        k_big<1024, false, S, true, false><<<grid, 1024, sm16, s>>>(a, tw, score);
       } else {
         set_error("weighted graph with big-tier degrees above %d", kBigMaxWeighted);
         return GLP_EINVAL;

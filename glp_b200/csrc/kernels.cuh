@@ -26,6 +26,8 @@
 // thread keeps only its best candidate and one reduction finishes the vertex,
 // independent of the order of the atomics: results are deterministic.
 #pragma once
+#include <type_traits>
+
 #include "device.cuh"
 
 namespace glp {
@@ -195,6 +197,8 @@ struct ScoreClassic {
   static __device__ __forceinline__ unsigned long long pack(const Best& b) {
     return ((unsigned long long)b.s << 32) | (uint32_t)b.l;
   }
+  // the monotone 32-bit key of a score (PackedCand)
+  __device__ __forceinline__ uint32_t key32(uint32_t k, int32_t) const { return k; }
   // the label of neighbour c (and, for scores that carry it, its volume)
   static constexpr bool kLV = false;
   __device__ __forceinline__ void load(const StepArgs& a, int32_t c, int32_t& lab, int32_t&) const {
@@ -260,6 +264,9 @@ struct ScoreLayered32 {
   __device__ __forceinline__ int64_t bound(uint32_t k) const { return (int64_t)(dstar * (int32_t)k); }
   static __device__ __forceinline__ unsigned long long pack(const Best& b) {
     return ((unsigned long long)((uint32_t)(int32_t)b.s ^ 0x80000000u) << 32) | (uint32_t)b.l;
+  }
+  __device__ __forceinline__ uint32_t key32(uint32_t k, int32_t v) const {
+    return (uint32_t)(dstar * (int32_t)k - v) ^ 0x80000000u;
   }
 };
 
@@ -405,17 +412,24 @@ __global__ void __launch_bounds__(256) k_group(StepArgs a, TierWork tw, S score)
 // shared atomicAdd stays cheap under moderate contention.  Called by all
 // lanes of the warp.
 // VIN: vl_in is the volume of lab, loaded with it (S::load of an S::kLV score).
-template <bool W, bool VIN = false, class S, class Ins>
+// merge (warp-uniform): fold lane 0's label as above; off, every lane adds
+// its own (measured faster in rows of mostly distinct labels, where the fold
+// rarely finds a copy).
+// B: Best, or PackedCand for S::kPacked scores.
+template <bool W, bool VIN = false, class S, class Ins, class B>
 __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, const S& score, const Ins& insert,
-                                            Best& best, bool& fail, bool scan = false, int32_t vl_in = 0) {
+                                            B& best, bool& fail, bool scan = false, int32_t vl_in = 0,
+                                            bool merge = true) {
   const int lane = threadIdx.x & 31;
-  const int32_t l0 = __shfl_sync(kFull, has ? lab : -1, 0);
-  const uint32_t m0 = __ballot_sync(kFull, has && lab == l0);
   uint32_t k = W ? wt : 1u;
-  if (l0 >= 0) {
-    const uint32_t k0 = W ? __reduce_add_sync(kFull, lab == l0 && has ? wt : 0u) : (uint32_t)__popc(m0);
-    if (lane == 0) k = k0;
-    else if (has && lab == l0) has = false;  // counted by lane 0
+  if (merge) {
+    const int32_t l0 = __shfl_sync(kFull, has ? lab : -1, 0);
+    const uint32_t m0 = __ballot_sync(kFull, has && lab == l0);
+    if (l0 >= 0) {
+      const uint32_t k0 = W ? __reduce_add_sync(kFull, lab == l0 && has ? wt : 0u) : (uint32_t)__popc(m0);
+      if (lane == 0) k = k0;
+      else if (has && lab == l0) has = false;  // counted by lane 0
+    }
   }
   if (!has) return;
   // the volume (S::kLV: loaded with the label) is in flight during the insert
@@ -424,8 +438,7 @@ __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, 
   if (tot == kNoSlot) {
     fail = true;
   } else if (!scan) {
-    const Best c{score.from_vol(tot, vl), lab};
-    if (better(c, best)) best = c;
+    offer(best, score, tot, vl, lab);
   }
 }
 
@@ -433,9 +446,10 @@ __device__ __forceinline__ void count_chunk(bool has, int32_t lab, uint32_t wt, 
 // t, t+stride, ... of it (scores with kScan).
 // Eight slots a round (four in kernels held to 40 registers), their volume
 // loads in flight together.
-template <bool C16 = false, class S>
+// CF: a claim-first table (table_claim_insert), whose vals hold count - 1.
+template <bool C16 = false, bool CF = false, class S, class B>
 __device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t* vals, uint32_t cap, uint32_t t,
-                                           uint32_t stride, const S& score, Best& best) {
+                                           uint32_t stride, const S& score, B& best) {
   constexpr int U = S::kSMThreads > 1024 ? 4 : 8;
   for (uint32_t s0 = t; s0 < cap; s0 += U * stride) {
     uint32_t key[U], val[U];
@@ -444,16 +458,13 @@ __device__ __forceinline__ void scan_table(const uint32_t* keys, const uint32_t*
     for (int u = 0; u < U; ++u) {
       const uint32_t s = s0 + u * stride;
       key[u] = s < cap ? keys[s] : 0u;
-      val[u] = s < cap ? count_at<C16>(vals, s) : 0u;
+      val[u] = s < cap ? (CF ? claim_count_at<C16>(keys, vals, s) : count_at<C16>(vals, s)) : 0u;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) vl[u] = key[u] ? score.vol_of((int32_t)(key[u] - 1u)) : 0;
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if (key[u]) {
-        const Best c{score.from_vol(val[u], vl[u]), (int32_t)(key[u] - 1u)};
-        if (better(c, best)) best = c;
-      }
+      if (key[u]) offer(best, score, val[u], vl[u], (int32_t)(key[u] - 1u));
   }
 }
 
@@ -531,6 +542,9 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
                                          : (C16 ? S::kSMThreads : S::kSMThreads == 2048 ? 1536 : 1024) / NT)
     k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
+  // unweighted 16-bit tables count claim-first; the lane-0 fold runs outside
+  // full-count steps, where listed vertices hold few distinct labels
+  constexpr bool CF = C16 && !W;
   const bool scan = S::kScan && scan_scores(a);
   __shared__ __align__(16) uint32_t skeys[NW][CAP];
   __shared__ __align__(16) uint32_t svals[NW][C16 ? CAP / 2 : CAP];
@@ -540,6 +554,7 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
   const int32_t stride = gridDim.x * NW;
+  const bool merge = !CF || mode != kModeFull;
   uint32_t* kk = skeys[warp];
   uint32_t* vv = svals[warp];
   // batch loader: columns (and weights) of entries j0 + 32q + lane below e,
@@ -593,10 +608,12 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
     zero_words16(kk, cap, lane, 32);
     zero_words16(vv, C16 ? cap / 2 : cap, lane, 32);
     __syncwarp();
-    Best best = best_none();
+    std::conditional_t<S::kPacked, PackedCand, Best> best{};
+    if constexpr (!S::kPacked) best = best_none();
     bool fail = false;
     auto ins = [&](uint32_t key, uint32_t k) {
-      return table_insert_bounded<C16>(kk, vv, cap - 1, key, k, cap, nullptr, nullptr);
+      return CF ? table_claim_insert<C16>(kk, vv, cap - 1, key, k, cap)
+                : table_insert_bounded<C16>(kk, vv, cap - 1, key, k, cap, nullptr, nullptr);
     };
     for (int32_t j0 = b; j0 < e; j0 += 128) {
       int32_t lab[4], vl[4];
@@ -613,18 +630,25 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + 32 * q < e) count_chunk<W, S::kLV>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, vl[q]);
+        if (j0 + 32 * q < e)
+          count_chunk<W, S::kLV>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, vl[q], merge);
     }
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {
       __syncwarp();
-      scan_table<C16>(kk, vv, cap, lane, 32, score, best);
+      scan_table<C16, CF>(kk, vv, cap, lane, 32, score, best);
     }
-    best = group_max<32>(best);
+    int32_t lbest;
+    if constexpr (S::kPacked) {
+      lbest = (int32_t)(uint32_t)warp_best(best);
+    } else {
+      best = group_max<32>(best);
+      lbest = best.l;
+    }
     bool chg = false;
     if (lane == 0) {
-      a.lout[v] = best.l;
-      chg = best.l != a.lcur[v];
+      a.lout[v] = lbest;
+      chg = lbest != a.lcur[v];
     }
     warp_note_change(a, cbuf[warp], ncb, chg, v);
     __syncwarp();  // the table is cleared for the next vertex
@@ -647,17 +671,23 @@ __device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32
 // ----------------------------------------------------------------- big tier
 // Exact count, one block per vertex: block shared table (dynamic) sized per
 // vertex to the power of two >= 2*degree.  C16 (unweighted counts only):
-// 16-bit counts, and at most kBig16Slots slots (three quarters full at
-// degree 24576), so 24576 labels fit 192 KB of shared memory.
+// claim-first 16-bit counts, and at most kBig16Slots slots (three quarters
+// full at degree 24576), so 24576 labels fit 192 KB of shared memory.
 // Unweighted blocks are held to S::kSMThreads threads per SM (classic: 32
 // registers, 32-bit layered: 40), weighted classic blocks of up to 512
 // threads to 40 (1536), which they fit without spilling; the other
 // instantiations to 64 (1024 threads per SM).
 constexpr uint32_t kBig16Slots = 32768;
-template <int NT, bool W, class S, bool C16 = false>
+// Rows above this degree fold lane 0's label in full-count steps too.
+constexpr int32_t kMergeDegree = 8192;
+// CF (with C16): claim-first inserts (table_claim_insert).  Off, a C16
+// table counts load-first; the top degree range runs so, its tables up to
+// three quarters full, where a CAS per probe measured slower.
+template <int NT, bool W, class S, bool C16 = false, bool CF = C16>
 __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 2048 && NT <= 512) ? 1536 : 1024) / NT)
     k_big(StepArgs a, TierWork tw, S score) {
   static_assert(!(C16 && W), "16-bit counts hold unweighted counts only");
+  static_assert(C16 || !CF, "claim-first tables are the 16-bit ones");
   const bool scan = S::kScan && scan_scores(a);
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ int32_t cbuf[64];  // changed vertices not yet listed (thread 0's)
@@ -723,11 +753,18 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
     zero_words16(smem, words, threadIdx.x, NT);  // degree > 32: cap >= 128
     if (S::kPacked && threadIdx.x == 0) sbest[par] = 0ull;
     __syncthreads();
-    Best best = best_none();
+    std::conditional_t<S::kPacked, PackedCand, Best> best{};
+    if constexpr (!S::kPacked) best = best_none();
     bool fail = false;
     auto ins = [&](uint32_t key, uint32_t k) {
-      return table_insert_bounded<C16>(keys, vals, cap - 1, key, k, cap, nullptr, nullptr);
+      return CF ? table_claim_insert<C16>(keys, vals, cap - 1, key, k, cap)
+                : table_insert_bounded<C16>(keys, vals, cap - 1, key, k, cap, nullptr, nullptr);
     };
+    // the lane-0 fold pays off on listed vertices (few distinct labels) and
+    // on the largest rows, where one label (a hub's own id, carried by its
+    // degree-1 neighbours) fills many lanes of a chunk: without it those
+    // lanes' adds to one slot serialise
+    const bool merge = !CF || mode != kModeFull || (e - b) > kMergeDegree;
     for (int32_t j0 = b + warp * 32; j0 < e; j0 += 4 * NT) {
       int32_t lab[4], vl[4];
       uint32_t wt[4];
@@ -742,26 +779,28 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
         if (lab[q] >= 0) score.load(a, lab[q], lab[q], vl[q]);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (j0 + q * NT < e) count_chunk<W, S::kLV>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, vl[q]);
+        if (j0 + q * NT < e)
+          count_chunk<W, S::kLV>(lab[q] >= 0, lab[q], wt[q], score, ins, best, fail, scan, vl[q], merge);
     }
     if (fail) atomicOr(a.err, kErrProbe);
     if (scan) {  // block-uniform
       __syncthreads();
-      scan_table<C16>(keys, vals, cap, threadIdx.x, NT, score, best);
+      scan_table<C16, CF>(keys, vals, cap, threadIdx.x, NT, score, best);
     }
-    if (S::kPacked) {
-      // S::pack is monotone in (score, label) and never 0 for a candidate
-      best = group_max<32>(best);
-      if (lane == 0 && best.l >= 0) atomicMax(&sbest[par], S::pack(best));
+    int32_t lbest = 0;
+    if constexpr (S::kPacked) {
+      // (key << 32 | label) is monotone in (score, label)
+      const unsigned long long wb = warp_best(best);
+      if (lane == 0 && wb) atomicMax(&sbest[par], wb);
       __syncthreads();
-      if (threadIdx.x == 0) best.l = (int32_t)(uint32_t)sbest[par];
+      if (threadIdx.x == 0) lbest = (int32_t)(uint32_t)sbest[par];
       par ^= 1;
     } else {
-      best = block_max<NT>(best, red);
+      lbest = block_max<NT>(best, red).l;
     }
     if (threadIdx.x == 0) {
-      a.lout[v] = best.l;
-      if (best.l != a.lcur[v]) {
+      a.lout[v] = lbest;
+      if (lbest != a.lcur[v]) {
         cbuf[ncb++] = v;
         if (ncb == 64) flush_big_changes(a, cbuf, ncb);
       }
