@@ -317,15 +317,24 @@ def run_reference(args, ws, rank):
     print(json.dumps(line))
 
 
-def full_count_roofline(plan: dict, runs: list, n: int, peak: float) -> dict:
+# the engine's default step-mode thresholds (glp_params majority_permille /
+# frontier_permille left at 0): a step after the first counts every vertex
+# only when the previous step changed at least this many labels per 1000
+# vertices (the rule of k_step_mode)
+MAJORITY_PERMILLE = 500
+
+
+def full_count_roofline(plan: dict, runs: list, n: int, peak: float,
+                        majority_permille: int = MAJORITY_PERMILLE) -> dict:
     """Roofline of the dominant kernel group over the steps that count every
     vertex of the group.  A classic step after the first runs in full mode
-    unless the previous step changed fewer than n/4 labels (then only the
-    vertices that fail a majority test, or below n/20 only the neighbours of
-    changed vertices, are recounted); the first step of a graph with ascending
-    rows is a closed form and launches no tier kernel.  Bytes per launch are
-    the group's algorithmic bytes, 8 per CSR entry (column + neighbour label)
-    and 12 per vertex (offsets, own label, written label)."""
+    unless the previous step changed fewer than majority_permille labels per
+    1000 vertices (then only the vertices that fail a majority test, or in
+    frontier steps only the neighbours of changed vertices, are recounted);
+    the first step of a graph with ascending rows is a closed form and
+    launches no tier kernel.  Bytes per launch are the group's algorithmic
+    bytes, 8 per CSR entry (column + neighbour label) and 12 per vertex
+    (offsets, own label, written label)."""
     per = {}
     full_steps = 0
     for r in runs:
@@ -334,7 +343,7 @@ def full_count_roofline(plan: dict, runs: list, n: int, peak: float) -> dict:
         if st is None:
             continue
         for it in range(1, len(ch)):
-            if ch[it - 1] * 4 < n:
+            if int(ch[it - 1]) * 1000 < majority_permille * n:
                 continue
             full_steps += 1
             for t, key in TIER_PLAN_KEYS.items():

@@ -57,3 +57,34 @@ def test_host_rmat_csr_equals_engine_sampler_csr():
         o2, c2, _ = graphs.rmat(scale, 16, seed=seed, device="cpu").numpy()
         np.testing.assert_array_equal(off, o2)
         np.testing.assert_array_equal(cols, c2)
+
+
+def test_full_count_roofline_counts_only_full_steps():
+    """The full-count roofline averages a tier over the steps the engine runs
+    in full mode: a step follows one that changed at least majority_permille
+    labels per 1000 vertices (k_step_mode).  The changed counts below are
+    those of R-MAT scale 24, 20 iterations: steps 1-3 are full, step 4 (after
+    49.4 % changes) is a majority step."""
+    from types import SimpleNamespace
+
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    n = 16777216
+    changed = np.array([8871861, 8871861, 8849431, 8286877, 3338088, 54466] + [9737] * 14)
+    st = np.zeros((20, 8), dtype=np.float32)
+    st[1:4, 4] = 2.5   # big tier in the full steps
+    st[4, 4] = 0.04    # majority step: listed vertices only
+    st[1:4, 3] = 1.0
+    plan = {f"v_{k}": 1 for k in ("tiny", "group16", "group32", "mid", "big", "hub")}
+    plan.update({f"e_{k}": 10 for k in ("tiny", "group16", "group32", "mid", "big", "hub")})
+    run = SimpleNamespace(changed=changed, step_tier_ms=st)
+    roof = bench.full_count_roofline(plan, [run], n, 6450.0)
+    assert roof["full_count_launches"] == 3
+    assert roof["kernel"] == "k_big"
+    assert abs(roof["avg_launch_ms"] - 2.5) < 1e-6
+    # with the old quarter-of-n rule the majority step would have been counted
+    roof25 = bench.full_count_roofline(plan, [run], n, 6450.0, majority_permille=250)
+    assert roof25["full_count_launches"] == 4
