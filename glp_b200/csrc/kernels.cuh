@@ -704,12 +704,15 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
   for (int32_t i = blockIdx.x; i < nwork; i += gridDim.x) {
     const int32_t v = tw.at(mode, i);
     const int32_t b = a.off[v], e = a.off[v + 1];
+    // the vertex's own label, loaded here so that thread 0 does not wait for
+    // it after the reduction barrier while the block waits for thread 0
+    const int32_t cur = a.lcur[v];
     if (S::kMajority && mode == kModeFrontier) {
       // a frontier vertex of this tier has many neighbours and usually keeps
       // its label: a strict majority of its own label decides it without a
       // table (the majority pre-pass does this for every tier in majority
       // steps)
-      const int32_t cand = a.lcur[v];
+      const int32_t cand = cur;
       if (threadIdx.x == 0) msum[mpar][0] = msum[mpar][1] = 0u;
       __syncthreads();
       uint32_t cnt = 0, tot = 0;
@@ -800,7 +803,7 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
     }
     if (threadIdx.x == 0) {
       a.lout[v] = lbest;
-      if (lbest != a.lcur[v]) {
+      if (lbest != cur) {
         cbuf[ncb++] = v;
         if (ncb == 64) flush_big_changes(a, cbuf, ncb);
       }
