@@ -497,7 +497,14 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
       nv_c = a.lcur[nv_v];
     }
     uint32_t cnt = 0, tot = 0;
-    for (int32_t j0 = b + lane; j0 < e; j0 += 32 * U) {
+    // unweighted rows stop at the first chunk after which the own label's
+    // count proves a strict majority (2 cnt > d) or rules it out (even every
+    // unread entry could not lift it above d / 2): the answer is the same as
+    // after the whole row, and a formed community's big rows are decided
+    // after a little more than half of their entries
+    const uint32_t d = (uint32_t)(e - b);
+    for (int32_t c0 = b; c0 < e; c0 += 32 * U) {  // warp-uniform chunks
+      const int32_t j0 = c0 + lane;
       int32_t c[U];
       uint32_t wt[U];
 #pragma unroll
@@ -512,9 +519,17 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
         cnt += l == cand ? wt[q] : 0u;
         tot += wt[q];
       }
+      if (!W && c0 + 32 * U < e) {
+        const uint32_t seen = (uint32_t)(c0 + 32 * U - b);
+        const uint32_t sc = __reduce_add_sync(kFull, cnt);
+        if (2ull * sc > d || 2ull * (sc + (d - seen)) <= d) {
+          cnt = lane == 0 ? sc : 0u;  // the reduction below returns sc
+          break;
+        }
+      }
     }
     cnt = __reduce_add_sync(kFull, cnt);
-    tot = W ? __reduce_add_sync(kFull, tot) : (uint32_t)(e - b);
+    tot = W ? __reduce_add_sync(kFull, tot) : d;
     if (lane == 0) {
       if (2ull * cnt > (unsigned long long)tot) {
         a.lout[v] = cand;
