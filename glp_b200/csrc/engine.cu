@@ -370,7 +370,8 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
         (g->d_w && ((rc = zeroed(&p, (size_t)hp.hub_labels, &h.hw)) ||
                     (rc = zeroed(&p, (size_t)hp.hub_labels, &h.hsw)))) ||
         (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_best)) ||
-        (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_cand)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_state))) {
+        (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_cand)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_state)) ||
+        (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_lbl)) || (rc = zeroed(&p, (size_t)p.n_hubs, &h.hub_lb))) {
       free_plan(&p);
       return rc;
     }
@@ -477,8 +478,9 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
     const unsigned grid = (unsigned)std::min<int64_t>(p.n_chunks, kMaxGrid);
     const unsigned hgrid = (unsigned)cdiv(p.n_hubs, 256);
     if (L.allow_majority && modal) {
+      k_hub_bound<W><<<hgrid, 256, 0, L.aux[0]>>>(a, p.hub, L.prev_changed, L.hub_bound ? 1 : 0);
       k_hub_majority<kHubNT, W><<<grid, kHubNT, 0, L.aux[0]>>>(a, p.hub, p.n_chunks);
-      ++*launches;
+      *launches += 2;
     }
     k_hub_decide<<<hgrid, 256, 0, L.aux[0]>>>(a, p.hub);
     GLP_CUDA(cudaMemsetAsync(p.hub.bcnt, 0, sizeof(uint32_t) * p.hub.nitems, L.aux[0]));
@@ -946,6 +948,9 @@ static int run_classic(RunCtx& c, int32_t niter) {
   }
   const uint32_t cyc_cap = (uint32_t)std::max<int64_t>(1024, g->n / 8);
   const unsigned cyc_grid = (unsigned)device_sms() * 4;
+  // hub count bounds belong to this run's labels (an earlier run, SLPA's
+  // spoken labels among them, may have left its own)
+  if (g->plan.n_hubs) GLP_CUDA(cudaMemsetAsync(g->plan.hub.hub_lbl, 0xff, sizeof(int32_t) * g->plan.n_hubs, c.s));
   for (int32_t it = 0; it < niter; ++it) {
     set_l2_window(c, g->d_lab[it & 1]);
     const bool fr = g->symmetric == 1;
@@ -958,6 +963,7 @@ static int run_classic(RunCtx& c, int32_t niter) {
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;
     L.allow_majority = 1;
     L.allow_frontier = fr;
+    L.hub_bound = true;
     if (fr && it > 0) {
       L.front = p.front;
       L.front.epoch = ++g->epoch;

@@ -865,12 +865,55 @@ struct HubPlan {
   int32_t nhubs, nitems, max_nb;
   unsigned long long* hub_best;  // [nhubs] packed best (0 = none)
   unsigned long long* hub_cand;  // [nhubs] (own-label weight << 32) + total weight
-  uint32_t* hub_state;           // [nhubs] 1 = decided by the majority pass this step
+  uint32_t* hub_state;           // [nhubs] 0 = count exactly this step; 1 = decided by the majority pass
+                                 // (or inactive); 2 = take the majority pass; 3 = decided by the count bound
+  int32_t* hub_lbl;              // [nhubs] label whose count hub_lb bounds (-1: none)
+  uint32_t* hub_lb;              // [nhubs] lower bound on that label's count among this step's input labels
 };
 
 // Bucket of a key: the high bits of its hash (table slots use the low bits).
 __device__ __forceinline__ uint32_t hub_bucket_of(uint32_t key, uint32_t nb) {
   return (uint32_t)(((unsigned long long)fmix32(key) * nb) >> 32);
+}
+
+// Before the majority pass of a majority or frontier step: every hub that
+// takes part gets state 2, unless the count bound decides it (state 3).
+// The bound (unweighted classic steps, `use`): the majority pass of an
+// earlier step counted label l = hub_lbl at c = hub_lb of the hub's
+// neighbours; a step changes prev_changed labels in all, so l's count among
+// the next step's input is at least c - prev_changed.  A hub still holding l
+// whose bound is a strict majority keeps l without reading its row (exact:
+// the majority argument holds for the bound, hence for the count).  Hubs
+// that no changed vertex touches (frontier state 1) keep both their label
+// and their count, so their bound stays as it is; a full step, whose hub
+// counts are not kept, clears every bound.
+template <bool W>
+__global__ void k_hub_bound(StepArgs a, HubPlan hp, const unsigned long long* prev_changed, int use) {
+  const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= hp.nhubs) return;
+  const int32_t mode = step_mode(a);
+  if (mode == kModeFull) {
+    hp.hub_lbl[h] = -1;
+    return;
+  }
+  if (mode == kModeFrontier && hp.hub_state[h] != 2u) return;
+  uint32_t st = 2u;
+  if (!W && use && prev_changed) {
+    const int32_t v = hp.hub_v[h];
+    const int32_t cand = a.lcur[v];
+    if (hp.hub_lbl[h] == cand) {
+      const unsigned long long chg = *prev_changed;
+      const uint32_t lb0 = hp.hub_lb[h];
+      const uint32_t lb = chg >= lb0 ? 0u : lb0 - (uint32_t)chg;
+      const uint32_t d = (uint32_t)(a.off[v + 1] - a.off[v]);
+      if (2ull * lb > d) {
+        hp.hub_lb[h] = lb;
+        a.lout[v] = cand;
+        st = 3u;
+      }
+    }
+  }
+  hp.hub_state[h] = st;
 }
 
 template <int NT, bool W>
@@ -881,7 +924,7 @@ __global__ void __launch_bounds__(NT) k_hub_majority(StepArgs a, HubPlan hp, int
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const int32_t h = hp.chunk_hub[c];
-    if (mode == kModeFrontier && hp.hub_state[h] != 2u) continue;  // block-uniform
+    if (hp.hub_state[h] != 2u) continue;  // block-uniform: inactive or decided by the bound
     const int32_t cand = a.lcur[hp.hub_v[h]];
     const int32_t cb = hp.chunk_begin[c], ce = hp.chunk_end[c];
     uint32_t cnt = 0, tot = 0;
@@ -921,20 +964,23 @@ __global__ void __launch_bounds__(NT) k_hub_majority(StepArgs a, HubPlan hp, int
 }
 
 // State after the step's majority pass: 1 = decided (or inactive), 0 = count
-// exactly.  In frontier mode only hubs marked active (state 2) take part.
+// exactly.  Outside full steps only hubs in state 2 took the pass; the
+// others keep state 1 or 3.  The pass's count is kept for k_hub_bound.
 __global__ void k_hub_decide(StepArgs a, HubPlan hp) {
   const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= hp.nhubs) return;
   const int32_t mode = step_mode(a);
-  if (mode == kModeFrontier && hp.hub_state[h] != 2u) return;  // inactive: keeps state 1
+  if (mode != kModeFull && hp.hub_state[h] != 2u) return;
+  const int32_t v = hp.hub_v[h];
   bool major = false;
   if (mode != kModeFull) {
     const unsigned long long p = hp.hub_cand[h];
     hp.hub_cand[h] = 0ull;
     const uint32_t kc = (uint32_t)(p >> 32), kt = (uint32_t)(p & 0xffffffffull);
     major = 2ull * kc > (unsigned long long)kt;
+    hp.hub_lbl[h] = a.lcur[v];
+    hp.hub_lb[h] = kc;
   }
-  const int32_t v = hp.hub_v[h];
   if (major) a.lout[v] = a.lcur[v];
   hp.hub_state[h] = major ? 1u : 0u;
 }
