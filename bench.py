@@ -840,7 +840,21 @@ def run_served(args, ws, rank, local):
             c["share"] = round(c["service_s"] / total_s, 4)
             c["service_s"] = round(c["service_s"], 3)
         unbatched = sum(c["service_s"] for k, c in classes.items() if k != "planted-classic")
-        out.append({"rate": rate, "served": served, "sequential": seq,
+        # latency percentiles per class, served and sequential: where the
+        # served path gains or loses against one request at a time
+        by_class = {}
+        for r, ls, lq in zip(reqs, lat, lat_s):
+            key = ("planted" if r["g"].n <= 100000 else "rmat") + "-" + {1: "classic", 2: "layered", 3: "slpa"}[
+                r["method"]]
+            c = by_class.setdefault(key, {"served": [], "sequential": []})
+            c["served"].append(ls)
+            c["sequential"].append(lq)
+        latency_by_class = {k: {"requests": len(v["served"]), "served_p50_ms": round(_pct(v["served"], 50), 2),
+                                "served_p99_ms": round(_pct(v["served"], 99), 2),
+                                "sequential_p50_ms": round(_pct(v["sequential"], 50), 2),
+                                "sequential_p99_ms": round(_pct(v["sequential"], 99), 2)}
+                            for k, v in by_class.items()}
+        out.append({"rate": rate, "served": served, "sequential": seq, "latency_by_class": latency_by_class,
                     "throughput_vs_sequential": round(served["throughput"] / seq["throughput"], 2),
                     "labels_match_alone": same, "sequential_service_by_class": classes,
                     "bound_if_batched_classes_were_free": round(total_s / max(unbatched, 1e-9), 2)})

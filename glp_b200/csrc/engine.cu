@@ -337,6 +337,15 @@ static int ensure_plan(glp_graph* g, const TierParams& t) {
     free_plan(&p);
     return rc;
   }
+  if (p.big.n && !p.big.ids) {  // a contiguous big tier: count bounds for its frontier steps
+    if ((rc = zeroed(&p, (size_t)p.big.n, &p.bb.lbl)) || (rc = zeroed(&p, (size_t)p.big.n, &p.bb.lb)) ||
+        (rc = zeroed(&p, (size_t)p.big.n, &p.bb.nchg))) {
+      free_plan(&p);
+      return rc;
+    }
+    p.bb.base = p.big.base;
+    p.bb.n = p.big.n;
+  }
   g->epoch = 0;  // fresh marks
   g->cyc_tag = 0;
   p.fmid.count = p.counts;
@@ -948,9 +957,16 @@ static int run_classic(RunCtx& c, int32_t niter) {
   }
   const uint32_t cyc_cap = (uint32_t)std::max<int64_t>(1024, g->n / 8);
   const unsigned cyc_grid = (unsigned)device_sms() * 4;
-  // hub count bounds belong to this run's labels (an earlier run, SLPA's
-  // spoken labels among them, may have left its own)
+  // hub and big-tier count bounds belong to this run's labels (an earlier
+  // run, SLPA's spoken labels among them, may have left its own); the big
+  // tier's bounds serve unweighted exact-count runs
   if (g->plan.n_hubs) GLP_CUDA(cudaMemsetAsync(g->plan.hub.hub_lbl, 0xff, sizeof(int32_t) * g->plan.n_hubs, c.s));
+  BigBound bb{};
+  if (!W && c.backend == GLP_BACKEND_EXACT && g->plan.bb.n) {
+    bb = g->plan.bb;
+    GLP_CUDA(cudaMemsetAsync(bb.lbl, 0xff, sizeof(int32_t) * bb.n, c.s));
+    GLP_CUDA(cudaMemsetAsync(bb.nchg, 0, sizeof(uint32_t) * bb.n, c.s));
+  }
   for (int32_t it = 0; it < niter; ++it) {
     set_l2_window(c, g->d_lab[it & 1]);
     const bool fr = g->symmetric == 1;
@@ -958,6 +974,7 @@ static int run_classic(RunCtx& c, int32_t niter) {
     StepArgs a{g->d_off, g->d_cols, g->d_w, g->d_lab[it & 1], g->d_lab[it & 1], g->d_lab[(it + 1) & 1],
                g->d_changed + it, g->d_err, p.d_mode, g->n, fr ? p.chg[it & 1] : nullptr,
                fr ? p.counts + 7 + (it & 1) : nullptr};
+    a.bb = bb;
     if (fr) GLP_CUDA(cudaMemsetAsync(p.counts + 7 + (it & 1), 0, sizeof(uint32_t), c.s));
     StepLaunch L = c.launch();
     L.prev_changed = it > 0 ? g->d_changed + it - 1 : nullptr;

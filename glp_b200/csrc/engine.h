@@ -91,6 +91,7 @@ struct DevicePlan {
   int32_t n_hubs = 0, n_chunks = 0;
   int64_t isolated = 0;
   HubPlan hub{};
+  BigBound bb{};  // count bounds of a contiguous big tier (n = 0: the tier is an id list)
   std::vector<void*> allocs;
 };
 

@@ -32,6 +32,23 @@
 
 namespace glp {
 
+// Count bounds of a contiguous big tier, vertices base .. base+n-1 (n = 0:
+// off).  For big vertex base + i: lbl[i] is a label and lb[i] a lower bound
+// on its count among the current step's input labels (-1: none; written by
+// the majority pre-pass and the frontier majority test, cleared by full
+// steps); nchg[i] counts its neighbours changed by the previous step
+// (k_frontier_push adds them, the big-tier launch of the frontier step takes
+// and clears them).  Only unweighted classic runs set it: their gathered
+// labels are the current labels, and a changed neighbour moves a count by
+// at most one.
+struct BigBound {
+  int32_t* lbl = nullptr;
+  uint32_t* lb = nullptr;
+  uint32_t* nchg = nullptr;
+  int32_t base = 0, n = 0;
+  __device__ __forceinline__ bool has(int32_t v) const { return (uint32_t)(v - base) < (uint32_t)n; }
+};
+
 // Neighbour labels, own labels and the output of one step.
 struct StepArgs {
   const int32_t* off;
@@ -48,6 +65,7 @@ struct StepArgs {
   // vertices whose label changed this step are appended here (nullable)
   int32_t* chg_out;
   uint32_t* chg_out_n;
+  BigBound bb{};
 };
 
 // Counts (and, when a.chg_out is set, lists) the vertices whose label changed.
@@ -531,6 +549,12 @@ __global__ void __launch_bounds__(256) k_major_warp(StepArgs a, Verts vs, int32_
     cnt = __reduce_add_sync(kFull, cnt);
     tot = W ? __reduce_add_sync(kFull, tot) : d;
     if (lane == 0) {
+      // the count (partial after an early stop: still a lower bound) bounds
+      // the frontier step that may follow
+      if (!W && a.bb.has(v)) {
+        a.bb.lbl[v - a.bb.base] = cand;
+        a.bb.lb[v - a.bb.base] = cnt;
+      }
       if (2ull * cnt > (unsigned long long)tot) {
         a.lout[v] = cand;
       } else {
@@ -715,6 +739,7 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
   // i's result while the block already counts vertex i+1 into the other
   __shared__ unsigned long long sbest[2];
   __shared__ uint32_t msum[2][2];  // majority test: (own-label weight, total weight) per vertex parity
+  __shared__ uint32_t sdec[2];     // frontier vertex decided by its count bound, per vertex parity
   int par = 0, mpar = 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int32_t mode = step_mode(a);
@@ -731,8 +756,32 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
       // table (the majority pre-pass does this for every tier in majority
       // steps)
       const int32_t cand = cur;
-      if (threadIdx.x == 0) msum[mpar][0] = msum[mpar][1] = 0u;
+      if (threadIdx.x == 0) {
+        msum[mpar][0] = msum[mpar][1] = 0u;
+        // count bound: the last count of its label, less the neighbours
+        // that changed since, is still a strict majority -> keeps it unread
+        uint32_t dec = 0u;
+        if (!W && a.bb.has(v)) {
+          const int32_t bi = v - a.bb.base;
+          const uint32_t nc = a.bb.nchg[bi];
+          a.bb.nchg[bi] = 0u;
+          if (a.bb.lbl[bi] == cand) {
+            const uint32_t lb0 = a.bb.lb[bi];
+            const uint32_t lb = nc >= lb0 ? 0u : lb0 - nc;
+            if (2ull * lb > (unsigned long long)(e - b)) {
+              a.bb.lb[bi] = lb;
+              dec = 1u;
+            }
+          }
+        }
+        sdec[mpar] = dec;
+      }
       __syncthreads();
+      if (sdec[mpar]) {  // block-uniform
+        if (threadIdx.x == 0) a.lout[v] = cand;
+        mpar ^= 1;
+        continue;
+      }
       uint32_t cnt = 0, tot = 0;
       for (int32_t j0 = b + threadIdx.x; j0 < e; j0 += 4 * NT) {
         int32_t c[4];
@@ -757,12 +806,18 @@ __global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 20
       }
       __syncthreads();
       const bool major = 2ull * msum[mpar][0] > (unsigned long long)msum[mpar][1];
+      if (!W && threadIdx.x == 0 && a.bb.has(v)) {  // the exact count of this step's input
+        a.bb.lbl[v - a.bb.base] = cand;
+        a.bb.lb[v - a.bb.base] = msum[mpar][0];
+      }
       mpar ^= 1;  // the next vertex resets the other pair while this one is read
       if (major) {  // block-uniform
         if (threadIdx.x == 0) a.lout[v] = cand;
         continue;
       }
     }
+    // a full-count step keeps no own-label count: the bounds go stale
+    if (!W && mode == kModeFull && threadIdx.x == 0 && a.bb.has(v)) a.bb.lbl[v - a.bb.base] = -1;
     // two slots a neighbour (four, where a launch's table had room for them,
     // measured no faster in this tier)
     const uint32_t cap = C16 ? min(pow2_ceil(2u * (uint32_t)(e - b)), kBig16Slots) : pow2_ceil(2u * (uint32_t)(e - b));
@@ -1359,6 +1414,7 @@ __global__ void __launch_bounds__(256) k_frontier_push(StepArgs a, Frontier f) {
       int32_t x = 0;
       if (j < e) {
         x = ld_stream(a.cols + j);
+        if (a.bb.has(x)) atomicAdd(a.bb.nchg + (x - a.bb.base), 1u);
         if (atomicExch(f.act + x, f.epoch) != f.epoch) {
           const int32_t d = a.off[x + 1] - a.off[x];
           tier = d <= f.tiny_max ? 0 : d <= 16 ? 1 : d <= 32 ? 2 : d <= f.mid_max ? 3 : d <= f.big_max ? 4 : -1;
