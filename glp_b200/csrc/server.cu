@@ -126,6 +126,10 @@ struct glp_server {
   bool stopping = false;
   std::vector<std::thread> threads;
   std::atomic<int64_t> rounds{0};
+  // one-graph solves running on the worker threads: while one holds the
+  // GPU, a batched round takes a grid sized to itself (it can start beside
+  // the solve); otherwise every SM
+  std::atomic<int> solves{0};
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
@@ -216,6 +220,7 @@ struct OneGraphRunner {
   glp_server* s;
   std::unordered_map<int64_t, Cached> cache;
   bool urgent = false;  // handles on the device's highest stream priority
+  bool counted = false;  // a worker's runner: its solves show in glp_server::solves
 
   void drop(int64_t id) {
     auto it = cache.find(id);
@@ -277,7 +282,9 @@ struct OneGraphRunner {
       glp_outputs out{};
       out.labels = r->labels;
       glp_graph_set_cancel_flag(g, &r->cancel);
+      if (counted) s->solves.fetch_add(1);
       rc = glp_run(g, r->method, &r->params, r->niter, &out, nullptr, nullptr, nullptr);
+      if (counted) s->solves.fetch_sub(1);
       glp_graph_set_cancel_flag(g, nullptr);
     }
     const std::string err = rc ? glp_last_error() : std::string();
@@ -290,7 +297,7 @@ struct OneGraphRunner {
 // short worker (short_lane) serves short_q only, on urgent streams.
 void plain_worker(glp_server* s, bool short_lane) {
   cudaSetDevice(s->cfg.device);
-  OneGraphRunner one{s, {}, short_lane};
+  OneGraphRunner one{s, {}, short_lane, true};
   for (;;) {
     Request* r = nullptr;
     std::vector<int64_t> stale;
@@ -448,12 +455,14 @@ void batch_worker(glp_server* s) {
     }
     if (rc == GLP_OK) {
       packed.resize((size_t)std::max<int64_t>(total, 1));
-      // a grid sized to the round (one CTA per 8192 vertices, at least 8):
-      // a small round's CTAs can all become resident while a long one-graph
-      // solve still holds the rest of the GPU
+      // while a one-graph solve of a worker thread holds the GPU,
+      // a grid sized to the round (one CTA per 8192 vertices, at least 8),
+      // whose CTAs can all become resident beside the solve's blocks; on an
+      // otherwise idle GPU every SM (a lone graph of 10k-100k vertices on
+      // eight CTAs would use a twentieth of the GPU)
       glp_params bp;
       glp_params_default(&bp);
-      bp.batch_blocks = (int32_t)std::max<int64_t>(8, (total + 8191) / 8192);
+      bp.batch_blocks = s->solves.load() > 0 ? (int32_t)std::max<int64_t>(8, (total + 8191) / 8192) : 0;
       rc = glp_batch_run(b, &bp, GLP_BATCH_OWN_ITERATIONS, packed.data(), 0, nullptr, nullptr);
     }
     const std::string err = rc ? glp_last_error() : std::string();
