@@ -455,14 +455,17 @@ void batch_worker(glp_server* s) {
     }
     if (rc == GLP_OK) {
       packed.resize((size_t)std::max<int64_t>(total, 1));
-      // while a one-graph solve of a worker thread holds the GPU,
-      // a grid sized to the round (one CTA per 8192 vertices, at least 8),
-      // whose CTAs can all become resident beside the solve's blocks; on an
-      // otherwise idle GPU every SM (a lone graph of 10k-100k vertices on
-      // eight CTAs would use a twentieth of the GPU)
+      // while a one-graph solve of a worker thread holds the GPU, a grid
+      // sized to the round (one CTA per 8192 vertices, at least 8), whose
+      // CTAs can all become resident beside the solve's blocks; on an
+      // otherwise idle GPU one CTA per 1024 vertices (a lone graph of 10k-100k
+      // vertices on eight CTAs would use a twentieth of the GPU; on every SM
+      // it would hold the whole GPU, and a short solve arriving meanwhile
+      // would wait for the round)
       glp_params bp;
       glp_params_default(&bp);
-      bp.batch_blocks = s->solves.load() > 0 ? (int32_t)std::max<int64_t>(8, (total + 8191) / 8192) : 0;
+      bp.batch_blocks = (int32_t)std::min<int64_t>(
+          INT32_MAX, std::max<int64_t>(8, s->solves.load() > 0 ? (total + 8191) / 8192 : (total + 1023) / 1024));
       rc = glp_batch_run(b, &bp, GLP_BATCH_OWN_ITERATIONS, packed.data(), 0, nullptr, nullptr);
     }
     const std::string err = rc ? glp_last_error() : std::string();
