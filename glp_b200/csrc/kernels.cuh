@@ -725,8 +725,13 @@ constexpr int32_t kMergeDegree = 8192;
 // CF (with C16): claim-first inserts (table_claim_insert).  Off, a C16
 // table counts load-first; the top degree range runs so, its tables up to
 // three quarters full, where a CAS per probe measured slower.
+// 1024-thread blocks of packed scores run two to an SM at 32 registers; the
+// 32-bit layered score spills there (36-52 bytes) and still measured faster
+// than one block at 64 (layered R-MAT s24 big tier 2.88 -> 2.70 ms per
+// iteration)
 template <int NT, bool W, class S, bool C16 = false, bool CF = C16>
-__global__ void __launch_bounds__(NT, (!W ? S::kSMThreads : (S::kSMThreads == 2048 && NT <= 512) ? 1536 : 1024) / NT)
+__global__ void __launch_bounds__(NT, (!W ? ((NT == 1024 && S::kPacked) ? 2048 : S::kSMThreads)
+                                          : (S::kSMThreads == 2048 && NT <= 512) ? 1536 : 1024) / NT)
     k_big(StepArgs a, TierWork tw, S score) {
   static_assert(!(C16 && W), "16-bit counts hold unweighted counts only");
   static_assert(C16 || !CF, "claim-first tables are the 16-bit ones");
