@@ -70,7 +70,8 @@ class Params(C.Structure):
         ("serial_step", C.c_int32),
         ("mid_prefetch", C.c_int32),
         ("batch_blocks", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("big_staged", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

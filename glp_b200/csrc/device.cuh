@@ -13,7 +13,48 @@ enum : uint32_t {
   kErrScoreRange = 2u,  // a layered score left the packable range
   kErrHubPlan = 4u,     // hub chunk bookkeeping inconsistent
   kErrTable = 8u,       // a vertex's table would not fit the launch's shared memory
+  kErrWait = 16u,       // a bounded wait on a bulk copy's mbarrier ran out
 };
+
+// Bulk global -> shared copies (cp.async.bulk, no multicast: this GPU's own
+// memory only) completing on a shared-memory mbarrier.  Source, destination
+// and size must be multiples of 16 bytes.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// Makes the initialised barriers visible to the bulk-copy (async) proxy.
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Orders this thread's earlier generic accesses to shared memory before
+// later bulk copies that write it.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for phase `parity` of the barrier to complete, at most ~2^20 polls
+// (well under a second); false when the wait ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 20); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it >= 32) __nanosleep(64);
+  }
+  return false;
+}
 
 // Dynamic shared memory of the running launch, in bytes.
 __device__ __forceinline__ uint32_t dynamic_smem_bytes() {

@@ -549,7 +549,16 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       const unsigned grid = (unsigned)std::min<int64_t>(vs.n, kMaxGrid);
       if (k16 && r < kBigParts - 1) {
         const size_t sm16 = 12ull * kBigPartMax[r];  // 2*max slots of 4 + 2 bytes
-        if (r <= 1) {
+        bool staged = false;
+        if constexpr (S::kPacked) {
+          if (r == 0 && L.big_staged && kBigPartMax[0] <= kStagedRow) {
+            // rows staged in shared memory by bulk copies, one vertex ahead
+            k_big_staged<256, S><<<grid, 256, sm16, s>>>(a, tw, score);
+            staged = true;
+          }
+        }
+        if (staged) {
+        } else if (r <= 1) {
           k_big<256, false, S, true><<<grid, 256, sm16, s>>>(a, tw, score);
         } else if (r == 2 && S::kSMThreads < 2048) {  // 40-register scores: 512 threads, three blocks per SM
           if ((rc = allow_smem(k_big<512, false, S, true>, sm16))) return rc;
@@ -657,6 +666,7 @@ struct RunCtx {
   uint32_t majority_pm = 500, frontier_pm = 50;  // glp_params step-mode thresholds
   bool l2_window = false;               // glp_params.l2_window
   bool mid_prefetch = true;             // glp_params.mid_prefetch
+  bool big_staged = false;              // glp_params.big_staged
   bool cycle = false;                   // stop a classic run once it ends in a two-step cycle
   int32_t cycle_from = -1;              // first iteration not run (the labels repeat from there)
 
@@ -700,6 +710,7 @@ struct RunCtx {
     L.majority_pm = majority_pm;
     L.frontier_pm = frontier_pm;
     L.mid_prefetch = mid_prefetch;
+    L.big_staged = big_staged;
     return L;
   }
   cudaEvent_t* current() { return timing && used ? evs[used - 1].data() : nullptr; }
@@ -743,7 +754,7 @@ static int check_err(glp_graph* g, cudaStream_t s) {
   if (err) {
     GLP_CUDA(cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), s));
     GLP_CUDA(cudaStreamSynchronize(s));
-    set_error("kernel error flags 0x%x (probe overflow=1, score range=2, hub plan=4, table past shared memory=8)",
+    set_error("kernel error flags 0x%x (probe overflow=1, score range=2, hub plan=4, table past shared memory=8, bulk-copy wait ran out=16)",
               err);
     return GLP_EKERNEL;
   }
@@ -1947,6 +1958,7 @@ int glp_run(glp_graph* g, int32_t method, const glp_params* pin, int32_t niter, 
   c.l2_window = p.l2_window != 0;
   c.cycle = !p.async && p.cycle_stop == 0;
   c.mid_prefetch = p.mid_prefetch == 0;
+  c.big_staged = p.big_staged > 0;
   c.timing = out->tier_ms != nullptr;
   GLP_CUDA(cudaMemsetAsync(g->d_changed, 0, sizeof(unsigned long long) * (total + 1), c.s));
   const bool W = g->d_w != nullptr;

@@ -113,6 +113,7 @@ struct StepLaunch {
   bool serial = false;  // every kernel on `stream` (per-tier timing without overlap)
   uint32_t majority_pm = 500, frontier_pm = 50;  // step-mode thresholds (changes per 1000 vertices)
   bool mid_prefetch = true;  // k_mid loads the next vertex's first batch while counting
+  bool big_staged = false;   // k_big_staged for the first big range of full-count steps
   // k_hub_bound may decide hubs from their earlier counts: classic steps,
   // whose gathered labels are the current labels (not SLPA's spoken ones)
   bool hub_bound = false;

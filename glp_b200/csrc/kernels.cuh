@@ -892,6 +892,127 @@ __global__ void __launch_bounds__(NT, (!W ? ((NT == 1024 && S::kPacked) ? 2048 :
   if (threadIdx.x == 0) flush_big_changes(a, cbuf, ncb);
 }
 
+// ------------------------------------------------------- big tier, staged
+// Full-count steps, degrees up to kStagedRow (one 256-thread block per
+// vertex, at most four entries a thread): the row's column segment is staged
+// in shared memory by one bulk copy (cp.async.bulk, completing on an
+// mbarrier), issued one vertex ahead into the other of two buffers, so the
+// next row's columns stream in while the block gathers and counts the
+// current one -- without holding them in registers.  The copy takes the
+// 16-byte-aligned superset of the row (the column array carries four pad
+// entries past m).  Counting is k_big's: claim-first 16-bit table, packed
+// candidates, no lane-0 fold (full-count rows of this range hold mostly
+// distinct labels).  Every mbarrier wait is bounded (kErrWait); after one
+// runs out a thread stops waiting, and at the end thread 0 waits, bounded,
+// for the copy it issued last.
+constexpr int32_t kStagedRow = 1024;
+constexpr uint32_t kStagedBuf = (uint32_t)kStagedRow + 8;  // ints: the aligned superset of a row
+
+template <int NT, class S>
+__global__ void __launch_bounds__(NT, S::kSMThreads / NT) k_big_staged(StepArgs a, TierWork tw, S score) {
+  static_assert(S::kPacked, "packed scores only");
+  constexpr int ITEMS = kStagedRow / NT;
+  extern __shared__ __align__(16) uint32_t smem[];  // table: 2*kStagedRow keys + their 16-bit counts
+  __shared__ __align__(128) int32_t scol[2][kStagedBuf];
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ unsigned long long sbest[2];
+  __shared__ int32_t cbuf[64];
+  uint32_t ncb = 0;
+  const int lane = threadIdx.x & 31;
+  const int32_t mode = step_mode(a);
+  const int32_t nwork = tw.size(mode);
+  if ((int32_t)blockIdx.x >= nwork) return;  // block-uniform, before any barrier exists
+  const bool scan = S::kScan && scan_scores(a);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+    sbest[0] = sbest[1] = 0ull;
+  }
+  __syncthreads();
+  // thread 0: stage the row of work item idx into buffer bi
+  auto issue = [&](int32_t idx, int bi) {
+    const int32_t u = tw.at(mode, idx);
+    const int32_t lo = a.off[u] & ~3, hi = (a.off[u + 1] + 3) & ~3;
+    const uint32_t bytes = (uint32_t)(hi - lo) * 4u;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&bar[bi], bytes);
+    bulk_copy_g2s(scol[bi], a.cols + lo, bytes, &bar[bi]);
+  };
+  if (threadIdx.x == 0) issue(blockIdx.x, 0);
+  uint32_t ph[2] = {0u, 0u};
+  bool waited_out = false;
+  // thread 0 after a wait ran out: the copies it left in flight (buffer,
+  // phase), waited for (bounded) before the block leaves; it issues no more
+  int pend_b[2] = {-1, -1};
+  uint32_t pend_p[2] = {0u, 0u};
+  int bi = 0, par = 0;
+  for (int32_t i = blockIdx.x; i < nwork; i += gridDim.x, bi ^= 1) {
+    const int32_t v = tw.at(mode, i);
+    const int32_t b = a.off[v], e = a.off[v + 1];
+    const int32_t cur = a.lcur[v];
+    if (threadIdx.x == 0 && a.bb.has(v)) a.bb.lbl[v - a.bb.base] = -1;  // a full-count step keeps no count
+    const uint32_t cap = pow2_ceil(2u * (uint32_t)(e - b));
+    uint32_t* keys = smem;
+    uint32_t* vals = smem + cap;
+    zero_words16(smem, cap + cap / 2, threadIdx.x, NT);  // degree > 32: cap >= 128
+    if (threadIdx.x == 0) sbest[par] = 0ull;
+    __syncthreads();  // every thread is done with the previous row and its buffer
+    const bool next = threadIdx.x == 0 && !waited_out && i + (int32_t)gridDim.x < nwork;
+    if (next) issue(i + gridDim.x, bi ^ 1);
+    if (!waited_out && !mbar_wait_bounded(&bar[bi], ph[bi])) {
+      waited_out = true;
+      atomicOr(a.err, kErrWait);
+      pend_b[0] = bi;
+      pend_p[0] = ph[bi];
+      if (next) {
+        pend_b[1] = bi ^ 1;
+        pend_p[1] = ph[bi ^ 1];
+      }
+    }
+    ph[bi] ^= 1u;
+    const int32_t lo = b & ~3;
+    int32_t lab[ITEMS], vl[ITEMS];
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+      const int32_t j = b + q * NT + (int32_t)threadIdx.x;
+      lab[q] = j < e ? scol[bi][j - lo] : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q)
+      if (lab[q] >= 0) score.load(a, lab[q], lab[q], vl[q]);
+    PackedCand best{};
+    bool fail = false;
+    auto ins = [&](uint32_t key, uint32_t k) { return table_claim_insert<true>(keys, vals, cap - 1, key, k, cap); };
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q)
+      if (b + q * NT + (threadIdx.x & ~31u) < (uint32_t)e)  // warp-uniform
+        count_chunk<false, S::kLV>(lab[q] >= 0, lab[q], 1u, score, ins, best, fail, scan, vl[q], false);
+    if (fail) atomicOr(a.err, kErrProbe);
+    if (scan) {  // block-uniform
+      __syncthreads();
+      scan_table<true, true>(keys, vals, cap, threadIdx.x, NT, score, best);
+    }
+    const unsigned long long wb = warp_best(best);
+    if (lane == 0 && wb) atomicMax(&sbest[par], wb);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int32_t l = (int32_t)(uint32_t)sbest[par];
+      a.lout[v] = l;
+      if (l != cur) {
+        cbuf[ncb++] = v;
+        if (ncb == 64) flush_big_changes(a, cbuf, ncb);
+      }
+    }
+    par ^= 1;
+  }
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2; ++k)
+      if (pend_b[k] >= 0) (void)mbar_wait_bounded(&bar[pend_b[k]], pend_p[k]);
+    flush_big_changes(a, cbuf, ncb);
+  }
+}
+
 // ----------------------------------------------------------------- hub tier
 // Vertices above the big tier.  Hub h gets nb_h = ceil(3*deg/kHubTable) hash
 // buckets, so a bucket averages at most kHubTable/3 labels and its distinct

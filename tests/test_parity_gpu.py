@@ -473,3 +473,27 @@ def test_prefetching_tier_kernels_keep_labels(case, pf):
     _, otr = O.classic_run(off, cols, niter, trace=True)
     for it in range(niter):
         np.testing.assert_array_equal(tr[it], otr[it], err_msg=f"iteration {it}")
+
+
+@pytest.mark.parametrize("method", [_lib.METHOD_CLASSIC, _lib.METHOD_LAYERED])
+def test_big_staged_rows_per_iteration(method):
+    """Full-count steps with the first big-tier range counted by
+    k_big_staged (each row's columns staged in shared memory by a bulk copy
+    issued one vertex ahead): labels after every iteration equal the
+    oracle's, on R-MAT scale 14, whose big tier holds degrees 257..1024."""
+    off, cols = CASES["rmat14"]
+    deg = np.diff(off)
+    assert ((deg >= 257) & (deg <= 1024)).sum() > 0
+    if method == _lib.METHOD_CLASSIC:
+        niter = 8
+        res, tr = _run_trace(off, cols, method, niter, big_staged=1)
+        _, otr = O.classic_run(off, cols, niter, trace=True)
+        np.testing.assert_array_equal(tr, otr)
+    else:
+        dstar = [2, 5, 17]
+        g = Graph(from_numpy(off, cols))
+        res = g.run(method, 3, make_params(dstar=dstar, big_staged=1))
+        g.close()
+        lab, vol = O.layered_run(off, cols, dstar, 3)
+        np.testing.assert_array_equal(res.labels, lab)
+        np.testing.assert_array_equal(res.vol, vol)
