@@ -582,7 +582,8 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
     k_mid(StepArgs a, TierWork tw, S score) {
   constexpr int NW = NT / 32;
   // unweighted 16-bit tables count claim-first; the lane-0 fold runs outside
-  // full-count steps, where listed vertices hold few distinct labels
+  // full-count steps, where listed vertices hold few distinct labels, and
+  // for classic-type scores in every step
   constexpr bool CF = C16 && !W;
   const bool scan = S::kScan && scan_scores(a);
   __shared__ __align__(16) uint32_t skeys[NW][CAP];
@@ -593,7 +594,11 @@ __global__ void __launch_bounds__(NT, PF ? (S::kPacked ? 1536 : 1024) / NT
   const int32_t mode = step_mode(a);
   const int32_t nwork = tw.size(mode);
   const int32_t stride = gridDim.x * NW;
-  const bool merge = !CF || mode != kModeFull;
+  // classic-type scores fold lane 0's label in full-count steps too (the
+  // third full-count step of R-MAT s24, whose labels have begun to gather,
+  // 1.12 -> 1.00 ms, the first two unchanged); the layered score does not
+  // (measured slower)
+  const bool merge = !CF || mode != kModeFull || S::kMajority;
   uint32_t* kk = skeys[warp];
   uint32_t* vv = svals[warp];
   // batch loader: columns (and weights) of entries j0 + 32q + lane below e,
