@@ -152,7 +152,7 @@ int tiers_for_graph(const glp_params* p, bool weighted, TierParams* t) {
     set_error("big_max %d above %d needs an unweighted graph (16-bit counts)", t->big_max, kBigMaxWeighted);
     return GLP_EINVAL;
   }
-  static_assert(kBigMaxWeighted <= kBigCap / 2, "weighted big tables hold 2*degree slots");
+  static_assert(4 * kBigMaxWeighted <= 3 * kBigCap, "a weighted big table is at most three quarters full");
   return GLP_OK;
 }
 
@@ -416,7 +416,7 @@ static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 // One launch over a device-built list of big-tier vertices (majority
 // failures, frontier members, screen fallbacks): 512-thread blocks with a
 // table for the tier's largest degree, with 16-bit counts on unweighted
-// graphs when the tier reaches past kBigMaxWeighted or the score packs
+// graphs when the tier reaches its last range (past 8192) or the score packs
 // (classic, 32-bit layered): smaller tables, more blocks per SM.
 template <bool W, class S>
 static int launch_big_list(const DevicePlan& p, const StepArgs& a, const TierWork& tw, const S& score,
@@ -575,13 +575,14 @@ int launch_step(const StepLaunch& Lin, const StepArgs& a, const S& score, int64_
       } else if (r == 3) {
         if ((rc = allow_smem(k_big<1024, W, S>, smr))) return rc;
         k_big<1024, W, S><<<grid, 1024, smr, s>>>(a, tw, score);
-      } else if constexpr (!W) {  // the 16-bit range: unweighted graphs only, load-first
+      } else if constexpr (!W) {  // the 16-bit range of unweighted graphs, load-first
         const size_t sm16 = (size_t)kBig16Slots * 6;
         if ((rc = allow_smem(k_big<1024, false, S, true, false>, sm16))) return rc;
         k_big<1024, false, S, true, false><<<grid, 1024, sm16, s>>>(a, tw, score);
-      } else {
-        set_error("weighted graph with big-tier degrees above %d", kBigMaxWeighted);
-        return GLP_EINVAL;
+      } else {  // weighted 8193..kBigMaxWeighted: 32-bit counts, kBigCap slots (128 KB)
+        const size_t smw = 2ull * kBigCap * sizeof(uint32_t);
+        if ((rc = allow_smem(k_big<1024, W, S>, smw))) return rc;
+        k_big<1024, W, S><<<grid, 1024, smw, s>>>(a, tw, score);
       }
       ++*launches;
     }

@@ -24,24 +24,26 @@ int device_sms();
 
 // Degree-tier parameters after defaults and limits are applied.
 // Exact-count tier limits: a mid warp's table holds kMidCap slots, a big
-// block's table kBigCap slots (both at most half full).
+// block's 32-bit table at most kBigCap slots (at most half full up to
+// degree 8192, three quarters at 12288).
 constexpr int kMidCap = 512, kBigCap = 16384;
 // In full mode the big tier runs as one launch per degree range: range r
 // holds degrees up to kBigPartMax[r] (and above the previous range), counted
 // by kBigPartThreads[r]-thread blocks whose tables hold 2*kBigPartMax[r]
 // slots, so that a range's table fits as many blocks per SM as it can.
-// The last range counts with 16-bit counts (k_big<..., C16>), so it exists
-// for unweighted graphs only: weighted graphs cap big_max at
-// kBigMaxWeighted.
+// The last range counts unweighted graphs with 16-bit counts (k_big<...,
+// C16>) up to 24576; weighted graphs count it with 32-bit counts in a
+// kBigCap-slot table (128 KB) and so cap big_max at kBigMaxWeighted.
 constexpr int kBigParts = 5;
 constexpr int kBigPartMax[kBigParts] = {1024, 2048, 4096, 8192, 24576};
 constexpr int kBigPartThreads[kBigParts] = {256, 256, 512, 1024, 1024};
-constexpr int kBigMaxWeighted = 8192, kBigMaxUnweighted = 24576;
+constexpr int kBigMaxWeighted = 12288, kBigMaxUnweighted = 24576;
+static_assert(kBigCap == (int)kBig32Slots, "the engine sizes 32-bit big tables as k_big caps them");
 
 struct TierParams {
   int32_t tiny_max = 8;       // <= 8
   int32_t mid_max = 256;      // <= kMidCap / 2
-  int32_t big_max = kBigMaxWeighted;  // <= kBigMaxUnweighted (unweighted graphs), <= kBigCap / 2 (weighted)
+  int32_t big_max = kBigMaxWeighted;  // <= kBigMaxUnweighted (unweighted graphs), <= kBigMaxWeighted (weighted)
   bool big_auto = true;               // big_max not given: the largest the graph's counts allow
   int32_t hub_chunk = 16384;  // edges per hub streaming block
   bool operator==(const TierParams& o) const {

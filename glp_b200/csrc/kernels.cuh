@@ -720,11 +720,13 @@ __device__ __forceinline__ void flush_big_changes(const StepArgs& a, const int32
 // vertex to the power of two >= 2*degree.  C16 (unweighted counts only):
 // claim-first 16-bit counts, and at most kBig16Slots slots (three quarters
 // full at degree 24576), so 24576 labels fit 192 KB of shared memory.
+// 32-bit tables hold at most kBig32Slots slots (three quarters full at
+// degree 12288, the weighted tier's largest): 128 KB.
 // Unweighted blocks are held to S::kSMThreads threads per SM (classic: 32
 // registers, 32-bit layered: 40), weighted classic blocks of up to 512
 // threads to 40 (1536), which they fit without spilling; the other
 // instantiations to 64 (1024 threads per SM).
-constexpr uint32_t kBig16Slots = 32768;
+constexpr uint32_t kBig16Slots = 32768, kBig32Slots = 16384;
 // Rows above this degree fold lane 0's label in full-count steps too.
 constexpr int32_t kMergeDegree = 8192;
 // CF (with C16): claim-first inserts (table_claim_insert).  Off, a C16
@@ -830,7 +832,7 @@ __global__ void __launch_bounds__(NT, (!W ? ((NT == 1024 && S::kPacked) ? 2048 :
     if (!W && mode == kModeFull && threadIdx.x == 0 && a.bb.has(v)) a.bb.lbl[v - a.bb.base] = -1;
     // two slots a neighbour (four, where a launch's table had room for them,
     // measured no faster in this tier)
-    const uint32_t cap = C16 ? min(pow2_ceil(2u * (uint32_t)(e - b)), kBig16Slots) : pow2_ceil(2u * (uint32_t)(e - b));
+    const uint32_t cap = min(pow2_ceil(2u * (uint32_t)(e - b)), C16 ? kBig16Slots : kBig32Slots);
     const uint32_t words = C16 ? cap + cap / 2 : 2 * cap;
     if (4ull * words > dynamic_smem_bytes()) {  // a planning error: report it, touch nothing (block-uniform)
       if (threadIdx.x == 0) atomicOr(a.err, kErrTable);

@@ -87,8 +87,8 @@ typedef struct glp_params {
   int32_t tiny_max;               /* thread per vertex up to this degree (<= 8) */
   int32_t mid_max;                /* warp per vertex up to this degree (32..256) */
   int32_t big_max;                /* block per vertex up to this degree (mid_max..24576 unweighted,
-                                     mid_max..8192 weighted); above: hubs.  0 = the largest the
-                                     graph allows (24576 unweighted, 8192 weighted) */
+                                     mid_max..12288 weighted); above: hubs.  0 = the largest the
+                                     graph allows (24576 unweighted, 12288 weighted) */
   int32_t hub_chunk;              /* edges per hub streaming block (256..65536) */
   int32_t use_graph;              /* capture the iteration loop in a CUDA graph */
   int32_t async;                  /* 1: enqueue on the stream and return without

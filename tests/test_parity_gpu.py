@@ -121,8 +121,12 @@ def test_layered_per_iteration(case, tier):
     np.testing.assert_array_equal(res.vol, vol)
 
 
-def test_layered_weighted():
-    off, cols = CASES["rmat12"]
+@pytest.mark.parametrize("case", ["rmat12", "ladder", "star_ring_10000"])
+def test_layered_weighted(case):
+    """Weighted layered steps, per step, labels and volumes; the ladder and
+    the 10000-leaf star put weighted vertices above degree 8192 in the big
+    tier's last range."""
+    off, cols = CASES[case]
     from glp_b200 import graphs
     w = graphs.add_weights(from_numpy(off, cols), 16, seed=3).weights.numpy()
     res, tr = _run_trace(off, cols, _lib.METHOD_LAYERED, 3, w=w, dstar=[2, 17])
@@ -324,15 +328,19 @@ def test_malformed_csr_rejected():
 
 def test_big_tier_bound_depends_on_weights():
     """Unweighted graphs count degrees up to 24576 in the big tier (16-bit
-    counts); weighted graphs stop at 8192, and reject a larger big_max."""
+    counts); weighted graphs stop at 12288 (32-bit counts), and reject a
+    larger big_max."""
     off, cols = CASES["star_ring_20000"]
     w = np.ones(len(cols), np.int32)
     with Graph(from_numpy(off, cols)) as g:
         assert g.plan()["v_hub"] == 0 and g.plan()["v_big"] == 1
+    off10, cols10 = CASES["star_ring_10000"]
+    with Graph(from_numpy(off10, cols10, np.ones(len(cols10), np.int32))) as g:
+        assert g.plan()["v_hub"] == 0 and g.plan()["v_big"] == 1
     with Graph(from_numpy(off, cols, w)) as g:
         assert g.plan()["v_hub"] == 1 and g.plan()["v_big"] == 0
         with pytest.raises(_lib.GlpError) as e:
-            g.run(_lib.METHOD_CLASSIC, 2, make_params(big_max=9000))
+            g.run(_lib.METHOD_CLASSIC, 2, make_params(big_max=12289))
         assert e.value.code == _lib.GLP_EINVAL
         res = g.run(_lib.METHOD_CLASSIC, 4)
     _, otr = O.classic_run(off, cols, 4, w=w, trace=True)
